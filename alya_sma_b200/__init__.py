@@ -1,0 +1,307 @@
+"""alya_sma_b200 -- B200 (sm_100a) explicit solid-mechanics step for
+superelastic shape-memory alloys: Alya solidz with constitutive law 160.
+
+Host-side mirror of the reference's interfaces over the C ABI of
+``libalya_sma_b200.so`` (declared in include/alya_sma.h):
+
+* ``eval_sld_stress_model_160`` -- the material plugin
+  (sld_stress_model_160.f90:36-195, flagt = 0) on a batch of Gauss points;
+* ``ExplicitSolid.assemble``    -- the explicit element loop
+  sld_matrix(SLD_EXPLICIT_SCHEME) (sld_matrix.f90:29-327) with host arrays;
+* ``ExplicitSolid.step``        -- the central-difference step sld_explicit
+  (mod_sld_solution_methods.f90:101-223) with BC update and state swap,
+  device resident and replayed as CUDA graphs.
+
+There is no CPU fallback: every call runs the CUDA library and raises
+``SmaError`` when it cannot (library missing, no sm_100 device, bad input).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import problem  # noqa: F401  (re-export)
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libalya_sma_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "alya_sma.h")
+
+PREC = {"fp64": 0, "fp32": 1}
+SCATTER = {"auto": 0, "atomic": 1, "color": 2}
+FIELD = {"displ": 0, "veloc": 1, "accel": 2, "rhsid": 3, "vmass": 4}
+COUNTERS = ["nr_active", "nr_failed", "nr_both", "neg_det", "nonfinite", "fallback64"]
+
+
+class SmaError(RuntimeError):
+    pass
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("nelem", C.c_int32), ("npoin", C.c_int32), ("lnods", C.c_void_p),
+                ("coord", C.c_void_p), ("lmate", C.c_void_p)]
+
+
+class _Mat(C.Structure):
+    _fields_ = [("nmate", C.c_int32), ("props", C.c_void_p), ("e_mart", C.c_void_p),
+                ("densi", C.c_void_p), ("tempe", C.c_void_p)]
+
+
+class _Run(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("scatter", C.c_int32), ("device", C.c_int32),
+                ("nfun", C.c_int32), ("dtime", C.c_double), ("fixno", C.c_void_p),
+                ("bcfun", C.c_void_p), ("fun_npts", C.c_void_p), ("fun_smooth", C.c_void_p),
+                ("fun_tab", C.c_void_p), ("fext", C.c_void_p), ("load_fun", C.c_int32),
+                ("block", C.c_int32)]
+
+
+class _Counters(C.Structure):
+    _fields_ = [("c", C.c_int64 * 8), ("gpdet_min", C.c_double)]
+
+
+_lib = None
+
+
+def header_functions() -> list[str]:
+    """Names of every entry point declared in include/alya_sma.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\*\s]+?\b(sma_\w+)\s*\(", txt, re.M)))
+
+
+def lib():
+    """Load the CUDA library (raises SmaError when it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SmaError(f"{LIB_PATH} is missing: run `python -m alya_sma_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.sma_last_error.restype = C.c_char_p
+        L.sma_version.restype = C.c_char_p
+        L.sma_stream.restype = C.c_void_p
+        L.sma_stream.argtypes = [C.c_void_p]
+        L.sma_kernel_launches.restype = C.c_int64
+        L.sma_kernel_launches.argtypes = [C.c_void_p]
+        L.sma_ctx_create.argtypes = [C.POINTER(_Mesh), C.POINTER(_Mat), C.POINTER(_Run), C.POINTER(C.c_void_p)]
+        L.sma_ctx_destroy.argtypes = [C.c_void_p]
+        L.sma_explicit_step.argtypes = [C.c_void_p, C.c_int32]
+        L.sma_assemble.argtypes = [C.c_void_p, C.c_void_p, C.c_double] + [C.c_void_p] * 5
+        L.sma_assemble_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        L.sma_end_step.argtypes = [C.c_void_p]
+        L.sma_eval_law160.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                      C.c_void_p]
+        L.sma_set_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.sma_get_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.sma_set_state.argtypes = [C.c_void_p, C.c_void_p]
+        L.sma_get_state.argtypes = [C.c_void_p, C.c_void_p]
+        L.sma_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.sma_set_time.argtypes = [C.c_void_p, C.c_double]
+        L.sma_get_counters.argtypes = [C.c_void_p, C.POINTER(_Counters)]
+        L.sma_reset_counters.argtypes = [C.c_void_p]
+        L.sma_set_witness.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+        L.sma_get_witness.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]
+        L.sma_critical_dt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.sma_set_timing.argtypes = [C.c_void_p, C.c_int32]
+        L.sma_get_timers.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise SmaError(f"alya_sma error {rc}: {lib().sma_last_error().decode()}")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+class ExplicitSolid:
+    """One explicit SMA solid on one GPU (a ``sma_ctx``).
+
+    ``prob`` is an ``alya_sma_b200.problem.Problem``.  precision "fp64" is the
+    reference's arithmetic; "fp32" runs element kinematics and the
+    constitutive update in FP32 (return map, force accumulation and time
+    integration stay FP64)."""
+
+    def __init__(self, prob, precision="fp64", scatter="atomic", device=0, dtime=None, block=0):
+        L = lib()
+        self.prob = prob
+        self.precision = precision
+        self.npoin, self.nelem = prob.npoin, prob.nelem
+        self._keep = dict(
+            lnods=_c(prob.lnods, np.int32), coord=_c(prob.coord, np.float64),
+            lmate=_c(prob.lmate, np.int32), props=_c(prob.props, np.float64),
+            e_mart=_c(prob.e_mart, np.float64), densi=_c(prob.densi, np.float64),
+            tempe=_c(prob.tempe, np.float64), fixno=_c(prob.fixno, np.int32),
+            bcfun=_c(prob.bcfun, np.int32), fun_npts=_c(prob.fun_npts, np.int32),
+            fun_smooth=_c(prob.fun_smooth, np.int32), fun_tab=_c(prob.fun_tab, np.float64),
+            fext=_c(prob.fext, np.float64))
+        k = self._keep
+        mesh = _Mesh(self.nelem, self.npoin, _p(k["lnods"]), _p(k["coord"]), _p(k["lmate"]))
+        mat = _Mat(k["props"].reshape(-1, 18).shape[0], _p(k["props"]), _p(k["e_mart"]),
+                   _p(k["densi"]), _p(k["tempe"]))
+        run = _Run(PREC[precision], SCATTER[scatter], device, int(k["fun_npts"].size),
+                   float(prob.dtime if dtime is None else dtime), _p(k["fixno"]), _p(k["bcfun"]),
+                   _p(k["fun_npts"]), _p(k["fun_smooth"]), _p(k["fun_tab"]), _p(k["fext"]),
+                   int(prob.load_fun), int(block))
+        self._ctx = C.c_void_p()
+        _check(L.sma_ctx_create(C.byref(mesh), C.byref(mat), C.byref(run), C.byref(self._ctx)))
+
+    def close(self):
+        if getattr(self, "_ctx", None) and self._ctx.value:
+            lib().sma_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- step boundary ------------------------------------------------------
+    def step(self, nsteps=1):
+        _check(lib().sma_explicit_step(self._ctx, int(nsteps)))
+
+    # -- element-loop boundary ----------------------------------------------
+    def assemble(self, displ, fext_scale=0.0, want_all=True):
+        """sld_matrix explicit: returns dict of (npoin,3) rhsid, finte, fexte,
+        frxid and (npoin,) vmass.  Reads state TIME_N, writes ITER_K."""
+        d = np.ascontiguousarray(displ, dtype=np.float64).reshape(self.npoin, 3)
+        out = {q: np.zeros((self.npoin, 3)) for q in ("rhsid", "finte", "fexte", "frxid")}
+        out["vmass"] = np.zeros(self.npoin)
+        if not want_all:
+            for q in ("finte", "fexte", "frxid", "vmass"):
+                out[q] = None
+        _check(lib().sma_assemble(self._ctx, _p(d), float(fext_scale), _p(out["rhsid"]),
+                                  _p(out["finte"]), _p(out["fexte"]), _p(out["frxid"]),
+                                  _p(out["vmass"])))
+        return out
+
+    def end_step(self):
+        _check(lib().sma_end_step(self._ctx))
+
+    # -- data ----------------------------------------------------------------
+    def get(self, field):
+        n = (self.npoin,) if field == "vmass" else (self.npoin, 3)
+        out = np.zeros(n)
+        _check(lib().sma_get_nodal(self._ctx, FIELD[field], _p(out)))
+        return out
+
+    def set(self, field, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.npoin, 3)
+        _check(lib().sma_set_nodal(self._ctx, FIELD[field], _p(a)))
+
+    @property
+    def state(self):
+        """svegm in the reference layout: (nelem, 2, 8, 3), slot 0 = ITER_K,
+        slot 1 = TIME_N."""
+        out = np.zeros((self.nelem, 2, 8, 3))
+        _check(lib().sma_get_state(self._ctx, _p(out)))
+        return out
+
+    @state.setter
+    def state(self, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.nelem, 2, 8, 3)
+        _check(lib().sma_set_state(self._ctx, _p(a)))
+
+    @property
+    def time(self):
+        t = C.c_double()
+        _check(lib().sma_get_time(self._ctx, C.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, t):
+        _check(lib().sma_set_time(self._ctx, float(t)))
+
+    def counters(self, reset=False):
+        c = _Counters()
+        _check(lib().sma_get_counters(self._ctx, C.byref(c)))
+        if reset:
+            _check(lib().sma_reset_counters(self._ctx))
+        return {name: int(c.c[i]) for i, name in enumerate(COUNTERS)}
+
+    def set_witness(self, dofs, max_steps):
+        d = np.ascontiguousarray(dofs, dtype=np.int32)
+        _check(lib().sma_set_witness(self._ctx, int(d.size), _p(d), int(max_steps)))
+        self._nwit = int(d.size)
+        self._wmax = int(max_steps)
+
+    def witness(self):
+        out = np.zeros((self._wmax, self._nwit))
+        n = C.c_int32()
+        _check(lib().sma_get_witness(self._ctx, _p(out), C.byref(n)))
+        return out[: n.value]
+
+    def critical_dt(self):
+        d = C.c_double()
+        _check(lib().sma_critical_dt(self._ctx, C.byref(d)))
+        return d.value
+
+    def set_timing(self, on=True):
+        _check(lib().sma_set_timing(self._ctx, int(bool(on))))
+
+    def timers(self):
+        """{'element': (ms, launches), 'nodal': (...), 'step': (...)} since
+        set_timing(True)."""
+        ms = np.zeros(3)
+        cnt = np.zeros(3, np.int64)
+        _check(lib().sma_get_timers(self._ctx, _p(ms), _p(cnt)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("element", "nodal", "step"))}
+
+    @property
+    def stream(self):
+        return lib().sma_stream(self._ctx)
+
+    @property
+    def kernel_launches(self):
+        return int(lib().sma_kernel_launches(self._ctx))
+
+
+def eval_sld_stress_model_160(props, gpgdi, gpsdv, gptmp=None, flagt=0, e_mart=0.0,
+                              precision="fp64"):
+    """Material plugin of law 160 on the GPU, batched.
+
+    Mirrors eval_sld_stress_model_160(pgaus, props, gpgdi, gptmp, gpsdv,
+    gpstr, gpdds, flagt) (sld_stress_model_160.f90:36-48) for any number of
+    Gauss points: ``gpgdi`` (n, 3, 3) deformation gradients with
+    gpgdi[g, i, j] = F(i, j); ``gpsdv`` (n, 3) state of slot TIME_N.  Returns
+    (gpstr (n, 3, 3) second Piola stress, new state (n, 3) for slot ITER_K,
+    NR flags (n,)).  Only flagt = 0 (explicit: no tangent) is provided.
+
+    Arrays may be numpy (copied through the device) or torch CUDA tensors
+    (used in place)."""
+    if flagt != 0:
+        raise SmaError("only flagt = 0 (explicit, no algorithmic tangent) is provided")
+    import torch
+    if not torch.cuda.is_available():
+        raise SmaError("eval_sld_stress_model_160 needs a CUDA device")
+    dev = torch.device("cuda")
+    F = torch.as_tensor(np.asarray(gpgdi) if not torch.is_tensor(gpgdi) else gpgdi,
+                        dtype=torch.float64, device=dev)
+    n = F.shape[0]
+    Fc = F.reshape(n, 3, 3).transpose(1, 2).contiguous()          # column-major per point
+    S0 = torch.as_tensor(np.asarray(gpsdv) if not torch.is_tensor(gpsdv) else gpsdv,
+                         dtype=torch.float64, device=dev).reshape(n, 3).contiguous()
+    T = None
+    if gptmp is not None:
+        T = torch.as_tensor(np.asarray(gptmp) if not torch.is_tensor(gptmp) else gptmp,
+                            dtype=torch.float64, device=dev).reshape(n).contiguous()
+    S1 = torch.empty_like(S0)
+    P = torch.empty((n, 9), dtype=torch.float64, device=dev)
+    fl = torch.empty(n, dtype=torch.int32, device=dev)
+    pr = np.ascontiguousarray(props, dtype=np.float64).reshape(18)
+    _check(lib().sma_eval_law160(n, _p(pr), float(e_mart), Fc.data_ptr(),
+                                 None if T is None else T.data_ptr(), S0.data_ptr(),
+                                 S1.data_ptr(), P.data_ptr(), fl.data_ptr(), PREC[precision],
+                                 torch.cuda.current_stream().cuda_stream))
+    torch.cuda.current_stream().synchronize()
+    gpstr = P.reshape(n, 3, 3).transpose(1, 2)
+    return gpstr, S1, fl

@@ -1,0 +1,938 @@
+// sma_capi.cu -- C ABI (include/alya_sma.h) of the B200 explicit SMA step:
+// context set-up, device buffers, CUDA-graph step loop, host I/O.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "alya_sma.h"
+#include "sma_kernels.cuh"
+
+using namespace sma;
+
+namespace {
+
+thread_local std::string g_err;
+
+int32_t fail(int32_t code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(SMA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename P>
+int32_t dalloc(P** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return SMA_OK;
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(SMA_ERR_NOMEM, std::string("cudaMalloc ") + std::to_string(bytes) + " bytes: " +
+                                   cudaGetErrorString(e));
+  }
+  return SMA_OK;
+}
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// host restatement of sld_elmmat.f90:199-209 summed per node in element
+// order (deterministic); FP64 geometry as jacobi.f90:172-219
+void host_lumped_mass(int nelem, const int32_t* lnods, const double* coord,
+                      const int32_t* lmate, const double* densi, std::vector<double>& vmass) {
+  const double p = 0.577350269189626;
+  double shp[8][8], der[8][24];
+  for (int g = 0; g < 8; ++g) {
+    const double s = (g & 4) ? p : -p, t = (g & 2) ? p : -p, z = (g & 1) ? p : -p;
+    const double sm = 0.5 * (1 - s), sq = 0.5 * (1 + s), tm = 0.5 * (1 - t), tp = 0.5 * (1 + t);
+    const double zm = 0.5 * (1 - z), zp = 0.5 * (1 + z), h = 0.5;
+    const double N[8] = {sm * tm * zm, sq * tm * zm, sq * tp * zm, sm * tp * zm,
+                         sm * tm * zp, sq * tm * zp, sq * tp * zp, sm * tp * zp};
+    const double d[24] = {-h * tm * zm, -h * sm * zm, -h * sm * tm, h * tm * zm, -h * sq * zm, -h * sq * tm,
+                          h * tp * zm,  h * sq * zm,  -h * sq * tp, -h * tp * zm, h * sm * zm, -h * sm * tp,
+                          -h * tm * zp, -h * sm * zp, h * sm * tm,  h * tm * zp, -h * sq * zp, h * sq * tm,
+                          h * tp * zp,  h * sq * zp,  h * sq * tp,  -h * tp * zp, h * sm * zp, h * sm * tp};
+    std::memcpy(shp[g], N, sizeof N);
+    std::memcpy(der[g], d, sizeof d);
+  }
+  for (int e = 0; e < nelem; ++e) {
+    const int32_t* ln = lnods + 8 * (int64_t)e;
+    const double rho = densi[lmate ? lmate[e] : 0];
+    for (int g = 0; g < 8; ++g) {
+      double xj[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < 8; ++k)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) xj[i + 3 * j] += coord[i + 3 * (int64_t)ln[k]] * der[g][j + 3 * k];
+      const double t1 = xj[4] * xj[8] - xj[5] * xj[7];
+      const double t2 = -xj[1] * xj[8] + xj[2] * xj[7];
+      const double t3 = xj[1] * xj[5] - xj[2] * xj[4];
+      const double vol = 1.0 * (xj[0] * t1 + xj[3] * t2 + xj[6] * t3);
+      for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b) vmass[ln[a]] += rho * vol * shp[g][a] * shp[g][b];
+    }
+  }
+}
+
+// critical time step (elmlen.f90 at the centre, natural length 2;
+// sld_velsnd.f90:117-124; mod_sld_minle_time_step.f90:262-268)
+double host_critical_dt(int nelem, const int32_t* lnods, const double* coord,
+                        const int32_t* lmate, const double* props, const double* e_mart,
+                        const double* densi) {
+  double dtcri = 1e300;
+  const double sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  for (int e = 0; e < nelem; ++e) {
+    const int32_t* ln = lnods + 8 * (int64_t)e;
+    double xj[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 8; ++k)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) xj[i + 3 * j] += coord[i + 3 * (int64_t)ln[k]] * 0.125 * sg[k][j];
+    const double t1 = xj[4] * xj[8] - xj[5] * xj[7];
+    const double t2 = -xj[1] * xj[8] + xj[2] * xj[7];
+    const double t3 = xj[1] * xj[5] - xj[2] * xj[4];
+    const double det = xj[0] * t1 + xj[3] * t2 + xj[6] * t3;
+    const double den = 1.0 / det;
+    double tr[9];
+    tr[0] = t1 * den; tr[1] = t2 * den; tr[2] = t3 * den;
+    tr[4] = (xj[0] * xj[8] - xj[2] * xj[6]) * den;
+    tr[5] = (-xj[0] * xj[5] + xj[3] * xj[2]) * den;
+    tr[8] = (xj[0] * xj[4] - xj[1] * xj[3]) * den;
+    tr[3] = (-xj[3] * xj[8] + xj[5] * xj[6]) * den;
+    tr[6] = (xj[3] * xj[7] - xj[4] * xj[6]) * den;
+    tr[7] = (-xj[0] * xj[7] + xj[1] * xj[6]) * den;
+    double hmin = 1e300;
+    for (int i = 0; i < 3; ++i) {
+      const double en = tr[i] * tr[i] + tr[i + 3] * tr[i + 3] + tr[i + 6] * tr[i + 6];
+      hmin = std::min(hmin, 2.0 / std::sqrt(en));
+    }
+    const int im = lmate ? lmate[e] : 0;
+    double young = props[18 * im];
+    if (e_mart && e_mart[im] > young) young = e_mart[im];
+    const double poiss = props[18 * im + 1];
+    const double lame1 = poiss * young / ((1.0 + poiss) * (1.0 - 2.0 * poiss));
+    const double lame2 = young / (2.0 * (1.0 + poiss));
+    const double velas = std::sqrt((lame1 + 2.0 * lame2) / densi[im]);
+    dtcri = std::min(dtcri, hmin / velas);
+  }
+  return dtcri;
+}
+
+// first-fit greedy colouring of elements sharing a node (the reference
+// colours the same graph, mod_parall_openmp.f90:557-708)
+int host_color(int nelem, int npoin, const int32_t* lnods, std::vector<int32_t>& order,
+               std::vector<int32_t>& cptr) {
+  std::vector<int32_t> cnt(npoin + 1, 0), adj(8 * (size_t)nelem), col(nelem, -1);
+  for (int64_t k = 0; k < 8 * (int64_t)nelem; ++k) cnt[lnods[k] + 1]++;
+  for (int p = 0; p < npoin; ++p) cnt[p + 1] += cnt[p];
+  std::vector<int32_t> pos(cnt.begin(), cnt.end());
+  for (int e = 0; e < nelem; ++e)
+    for (int a = 0; a < 8; ++a) adj[pos[lnods[8 * (int64_t)e + a]]++] = e;
+  int ncol = 0;
+  for (int e = 0; e < nelem; ++e) {
+    uint64_t used = 0;
+    for (int a = 0; a < 8; ++a) {
+      const int p = lnods[8 * (int64_t)e + a];
+      for (int k = cnt[p]; k < cnt[p + 1]; ++k) {
+        const int c = col[adj[k]];
+        if (c >= 0 && c < 64) used |= 1ull << c;
+      }
+    }
+    int c = 0;
+    while (c < 64 && ((used >> c) & 1)) ++c;
+    if (c >= 64) return -1;
+    col[e] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  cptr.assign(ncol + 1, 0);
+  for (int e = 0; e < nelem; ++e) cptr[col[e] + 1]++;
+  for (int c = 0; c < ncol; ++c) cptr[c + 1] += cptr[c];
+  std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+  order.resize(nelem);
+  for (int e = 0; e < nelem; ++e) order[fill[col[e]]++] = e;
+  return ncol;
+}
+
+MatC make_mat(const double* pr, double e_mart, double densi) {
+  MatC m;
+  std::memset(&m, 0, sizeof m);
+  const double E = pr[0], v = pr[1];
+  m.eL = pr[2];
+  m.alfa = pr[14];
+  m.C_AS = pr[5];
+  m.C_SA = pr[11];
+  m.K = E / (3.0 - 6.0 * v);
+  m.G = E / (2.0 + 2.0 * v);
+  const double aux = std::sqrt(2.0 / 3.0) + m.alfa;
+  m.Rf_AS = pr[4] * aux + m.C_AS * pr[6];
+  m.Rs_AS = pr[3] * aux + m.C_AS * pr[7];
+  m.Rf_SA = pr[10] * aux + m.C_SA * pr[12];
+  m.Rs_SA = pr[9] * aux + m.C_SA * pr[13];
+  m.G1 = (2.0 * m.G + 9.0 * (m.alfa * m.alfa) * m.K) * m.eL;
+  m.EA = E;
+  m.EM = (e_mart > 0.0) ? e_mart : E;
+  m.nu = v;
+  m.densi = densi;
+  m.ext_E = (e_mart > 0.0 && e_mart != E) ? 1 : 0;
+  return m;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct sma_ctx {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int prec = SMA_PREC_FP64;
+  int scatter = SMA_SCATTER_ATOMIC;
+  int block = 256;
+  int nelem = 0, npoin = 0;
+  int64_t npad = 0, sst = 0;
+  int nmate = 0;
+  // element order: internal position -> user element id (colour-sorted for
+  // SMA_SCATTER_COLOR, identity otherwise)
+  std::vector<int32_t> perm;
+  std::vector<int32_t> cptr;   // colour ranges (one range if ATOMIC)
+  // device
+  int32_t* d_lnods = nullptr;
+  int32_t* d_perm = nullptr;
+  int32_t* d_lmate = nullptr;
+  double* d_coord = nullptr;
+  double* d_u = nullptr;
+  double* d_vt = nullptr;
+  double* d_v = nullptr;
+  double* d_a = nullptr;
+  double* d_f = nullptr;
+  double* d_invm = nullptr;
+  double* d_fext = nullptr;
+  double* d_tempe = nullptr;
+  uint8_t* d_flags = nullptr;
+  int8_t* d_bcfun = nullptr;
+  MatC* d_mats = nullptr;
+  void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
+  int cur = 0;                             // state buffer holding TIME_N
+  unsigned long long* d_cnt = nullptr;
+  StepTime* d_ts = nullptr;
+  FunTab* d_ft = nullptr;
+  double* d_stage = nullptr;               // (3, npoin) staging for host I/O
+  double* d_stage2 = nullptr;
+  // witnesses
+  int nwit = 0, wit_max = 0;
+  int32_t* d_wdof = nullptr;
+  double* d_whist = nullptr;
+  int* d_wrow = nullptr;
+  // host copies
+  std::vector<double> vmass;
+  double dtcri = 0.0;
+  double dtime = 0.0;
+  bool has_load = false;
+  double grav[3] = {0, 0, 0};
+  // graphs: chunk of steps starting at state parity 0 / 1
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int gchunk = 0;
+  int64_t launches = 0;
+  // phase timers
+  bool timing = false;
+  double tms[3] = {0, 0, 0};
+  int64_t tcnt[3] = {0, 0, 0};
+  std::vector<cudaEvent_t> evpool;
+  std::vector<std::pair<int, std::pair<int, int>>> evmarks;  // (timer, (ev_begin, ev_end))
+  size_t evnext = 0;
+};
+
+namespace {
+
+template <typename T>
+ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance) {
+  ElemArgs<T> a;
+  a.lnods = c->d_lnods;
+  a.coord = c->d_coord;
+  a.u = c->d_u;
+  a.f = c->d_f;
+  a.lmate = c->d_lmate;
+  a.mats = c->d_mats;
+  a.tempe = c->d_tempe;
+  a.sold = (const T*)c->d_state[c->cur];
+  a.snew = (T*)c->d_state[c->cur ^ 1];
+  a.cnt = c->d_cnt;
+  a.ts = advance ? c->d_ts : nullptr;
+  a.ft = c->d_ft;
+  a.npad = c->npad;
+  a.sst = c->sst;
+  a.beg = beg;
+  a.end = end;
+  a.grav[0] = c->grav[0];
+  a.grav[1] = c->grav[1];
+  a.grav[2] = c->grav[2];
+  a.has_grav = (c->grav[0] != 0.0 || c->grav[1] != 0.0 || c->grav[2] != 0.0);
+  return a;
+}
+
+template <typename T>
+int32_t launch_elements_t(sma_ctx* c, bool advance) {
+  const int nrange = (int)c->cptr.size() - 1;
+  const int epb = c->block / 8;
+  const size_t smem = (size_t)epb * 9 * sizeof(ElemSmem<T>);
+  for (int r = 0; r < nrange; ++r) {
+    const int beg = c->cptr[r], end = c->cptr[r + 1];
+    if (end <= beg) continue;
+    ElemArgs<T> a = elem_args<T>(c, beg, end, advance && r == 0);
+    const unsigned grid = (unsigned)ceil_div(end - beg, epb);
+    if (c->scatter == SMA_SCATTER_COLOR)
+      k_element<T, false><<<grid, c->block, smem, c->stream>>>(a);
+    else
+      k_element<T, true><<<grid, c->block, smem, c->stream>>>(a);
+    c->launches++;
+  }
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+int32_t launch_elements(sma_ctx* c, bool advance) {
+  return c->prec == SMA_PREC_FP32 ? launch_elements_t<float>(c, advance)
+                                  : launch_elements_t<double>(c, advance);
+}
+
+NodalArgs nodal_args(sma_ctx* c) {
+  NodalArgs a;
+  a.u = c->d_u;
+  a.vt = c->d_vt;
+  a.v = c->d_v;
+  a.acc = c->d_a;
+  a.f = c->d_f;
+  a.invm = c->d_invm;
+  a.flags = c->d_flags;
+  a.bcfun = c->d_bcfun;
+  a.fext = c->d_fext;
+  a.ts = c->d_ts;
+  a.cnt = c->d_cnt;
+  a.npoin = c->npoin;
+  a.npad = c->npad;
+  return a;
+}
+
+int32_t launch_nodal(sma_ctx* c, int mode) {
+  const unsigned grid = (unsigned)ceil_div(c->npoin, 256);
+  NodalArgs a = nodal_args(c);
+  if (mode == 0) k_nodal<0><<<grid, 256, 0, c->stream>>>(a);
+  else if (mode == 1) k_nodal<1><<<grid, 256, 0, c->stream>>>(a);
+  else k_nodal<2><<<grid, 256, 0, c->stream>>>(a);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+int32_t launch_witness(sma_ctx* c) {
+  if (c->nwit <= 0) return SMA_OK;
+  k_witness<<<1, 128, 0, c->stream>>>(c->d_u, c->npad, c->d_wdof, c->nwit, c->d_whist,
+                                      c->d_wrow, c->wit_max);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+// one interior step: element loop (advancing time) + fused nodal update
+int32_t issue_step(sma_ctx* c, int nodal_mode) {
+  int32_t rc = launch_elements(c, true);
+  if (rc) return rc;
+  c->cur ^= 1;   // the state written by this step is TIME_N of the next
+  rc = launch_nodal(c, nodal_mode);
+  if (rc) return rc;
+  return launch_witness(c);
+}
+
+int32_t next_event(sma_ctx* c, int* idx) {
+  if (c->evnext == c->evpool.size()) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    c->evpool.push_back(e);
+  }
+  *idx = (int)c->evnext++;
+  CU(cudaEventRecord(c->evpool[*idx], c->stream));
+  return SMA_OK;
+}
+
+// timed variant of issue_step: events around the element loop, the nodal
+// update and the whole step
+int32_t issue_step_timed(sma_ctx* c, int nodal_mode) {
+  int e0, e1, e2, rc;
+  if ((rc = next_event(c, &e0))) return rc;
+  if ((rc = launch_elements(c, true))) return rc;
+  c->cur ^= 1;
+  if ((rc = next_event(c, &e1))) return rc;
+  if ((rc = launch_nodal(c, nodal_mode))) return rc;
+  if ((rc = next_event(c, &e2))) return rc;
+  c->evmarks.push_back({0, {e0, e1}});
+  c->evmarks.push_back({1, {e1, e2}});
+  c->evmarks.push_back({2, {e0, e2}});
+  return launch_witness(c);
+}
+
+int32_t collect_timers(sma_ctx* c) {
+  CU(cudaStreamSynchronize(c->stream));
+  for (auto& m : c->evmarks) {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, c->evpool[m.second.first], c->evpool[m.second.second]));
+    c->tms[m.first] += ms;
+    c->tcnt[m.first] += (m.first == 0) ? (int64_t)(c->cptr.size() - 1) : 1;
+  }
+  c->evmarks.clear();
+  c->evnext = 0;
+  return SMA_OK;
+}
+
+void destroy_graphs(sma_ctx* c) {
+  for (int p = 0; p < 2; ++p)
+    if (c->gexec[p]) {
+      cudaGraphExecDestroy(c->gexec[p]);
+      c->gexec[p] = nullptr;
+    }
+  c->gchunk = 0;
+}
+
+// capture `chunk` interior steps for both starting parities
+int32_t build_graphs(sma_ctx* c, int chunk) {
+  destroy_graphs(c);
+  const int saved = c->cur;
+  const int64_t saved_l = c->launches;
+  for (int p = 0; p < 2; ++p) {
+    c->cur = p;
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int32_t rc = SMA_OK;
+    for (int s = 0; s < chunk && rc == SMA_OK; ++s) rc = issue_step(c, 1);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); c->cur = saved; return rc; }
+    if (e != cudaSuccess) { c->cur = saved; return fail(SMA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
+    e = cudaGraphInstantiate(&c->gexec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { c->cur = saved; return fail(SMA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+  }
+  c->cur = saved;
+  c->launches = saved_l;
+  c->gchunk = chunk;
+  return SMA_OK;
+}
+
+int64_t kernels_per_step(const sma_ctx* c) {
+  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0);
+}
+
+template <typename T>
+int32_t alloc_state(sma_ctx* c) {
+  for (int s = 0; s < 2; ++s) {
+    int32_t rc = dalloc(&c->d_state[s], 3 * (size_t)c->sst * sizeof(T));
+    if (rc) return rc;
+    CU(cudaMemset(c->d_state[s], 0, 3 * (size_t)c->sst * sizeof(T)));
+  }
+  return SMA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sma_last_error(void) { return g_err.c_str(); }
+const char* sma_version(void) { return "alya_sma_b200 0.1 (sm_100a)"; }
+
+int32_t sma_ctx_destroy(sma_ctx* c) {
+  if (!c) return SMA_OK;
+  cudaSetDevice(c->dev);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  destroy_graphs(c);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_coord, c->d_u, c->d_vt, c->d_v, c->d_a,
+                  c->d_f, c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
+                  c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
+                  c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SMA_OK;
+}
+
+int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
+                       const sma_run_desc* run, sma_ctx** out) {
+  if (!out) return fail(SMA_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!mesh || !mat || !run) return fail(SMA_ERR_ARG, "NULL descriptor");
+  if (mesh->nelem <= 0 || mesh->npoin <= 0 || !mesh->lnods || !mesh->coord)
+    return fail(SMA_ERR_ARG, "empty mesh");
+  if (mat->nmate <= 0 || !mat->props || !mat->densi) return fail(SMA_ERR_ARG, "no material");
+  if (run->precision != SMA_PREC_FP64 && run->precision != SMA_PREC_FP32)
+    return fail(SMA_ERR_ARG, "precision must be SMA_PREC_FP64 or SMA_PREC_FP32");
+  if (run->nfun < 0 || run->nfun > MAXFUN) return fail(SMA_ERR_ARG, "at most 16 time functions");
+  if (run->block != 0 && (run->block % 32 != 0 || run->block < 32 || run->block > 256))
+    return fail(SMA_ERR_ARG, "block must be a multiple of 32 in [32, 256]");
+  for (int64_t k = 0; k < 8 * (int64_t)mesh->nelem; ++k)
+    if (mesh->lnods[k] < 0 || mesh->lnods[k] >= mesh->npoin)
+      return fail(SMA_ERR_ARG, "lnods entry out of range at " + std::to_string(k));
+  if (mesh->lmate)
+    for (int e = 0; e < mesh->nelem; ++e)
+      if (mesh->lmate[e] < 0 || mesh->lmate[e] >= mat->nmate)
+        return fail(SMA_ERR_ARG, "lmate entry out of range at " + std::to_string(e));
+  int nfun = run->nfun;
+  for (int f = 0; f < nfun; ++f)
+    if (run->fun_npts[f] < 1 || run->fun_npts[f] > MAXPTS)
+      return fail(SMA_ERR_ARG, "time function tables hold 1..32 rows");
+  if (run->bcfun)
+    for (int p = 0; p < mesh->npoin; ++p)
+      if (run->bcfun[p] >= nfun) return fail(SMA_ERR_ARG, "bcfun beyond nfun");
+  if (run->load_fun >= nfun) return fail(SMA_ERR_ARG, "load_fun beyond nfun");
+  for (int im = 0; im < mat->nmate; ++im) {
+    const double* pr = mat->props + 18 * im;
+    if (!(pr[0] > 0.0) || !(pr[1] > -1.0 && pr[1] < 0.5) || !(mat->densi[im] > 0.0))
+      return fail(SMA_ERR_ARG, "material " + std::to_string(im) + ": need E > 0, -1 < nu < 0.5, rho > 0");
+  }
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+    return fail(SMA_ERR_NODEVICE, "no CUDA device");
+  if (run->device < 0 || run->device >= ndev) return fail(SMA_ERR_ARG, "device ordinal");
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, run->device));
+  if (prop.major != 10) return fail(SMA_ERR_NODEVICE, "this build targets sm_100a (B200)");
+
+  sma_ctx* c = new sma_ctx();
+  int32_t rc = SMA_OK;
+#define TRY(x)                  \
+  do {                          \
+    rc = (x);                   \
+    if (rc) {                   \
+      sma_ctx_destroy(c);       \
+      return rc;                \
+    }                           \
+  } while (0)
+#define TRYCU(call)                                                                  \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      sma_ctx_destroy(c);                                                            \
+      return fail(SMA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    }                                                                                \
+  } while (0)
+
+  c->dev = run->device;
+  TRYCU(cudaSetDevice(c->dev));
+  TRYCU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->prec = run->precision;
+  c->scatter = (run->scatter == SMA_SCATTER_COLOR) ? SMA_SCATTER_COLOR : SMA_SCATTER_ATOMIC;
+  c->block = run->block ? run->block : 256;
+  c->nelem = mesh->nelem;
+  c->npoin = mesh->npoin;
+  c->npad = ceil_div(c->npoin, 32) * 32;
+  c->sst = ceil_div(8 * (int64_t)c->nelem, 32) * 32;
+  c->nmate = mat->nmate;
+  c->dtime = run->dtime;
+
+  // element order
+  c->perm.resize(c->nelem);
+  if (c->scatter == SMA_SCATTER_COLOR) {
+    int nc = host_color(c->nelem, c->npoin, mesh->lnods, c->perm, c->cptr);
+    if (nc < 0) { sma_ctx_destroy(c); return fail(SMA_ERR_ARG, "mesh needs more than 64 colours"); }
+  } else {
+    for (int e = 0; e < c->nelem; ++e) c->perm[e] = e;
+    c->cptr = {0, c->nelem};
+  }
+  std::vector<int32_t> lnods_i(8 * (size_t)c->nelem);
+  for (int e = 0; e < c->nelem; ++e)
+    std::memcpy(&lnods_i[8 * (size_t)e], mesh->lnods + 8 * (int64_t)c->perm[e], 8 * sizeof(int32_t));
+  TRY(dalloc(&c->d_lnods, lnods_i.size() * sizeof(int32_t)));
+  TRYCU(cudaMemcpy(c->d_lnods, lnods_i.data(), lnods_i.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  TRY(dalloc(&c->d_perm, c->perm.size() * sizeof(int32_t)));
+  TRYCU(cudaMemcpy(c->d_perm, c->perm.data(), c->perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (mesh->lmate && c->nmate > 1) {
+    std::vector<int32_t> lm(c->nelem);
+    for (int e = 0; e < c->nelem; ++e) lm[e] = mesh->lmate[c->perm[e]];
+    TRY(dalloc(&c->d_lmate, lm.size() * sizeof(int32_t)));
+    TRYCU(cudaMemcpy(c->d_lmate, lm.data(), lm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (mat->tempe) {
+    std::vector<double> tp(c->nelem);
+    for (int e = 0; e < c->nelem; ++e) tp[e] = mat->tempe[c->perm[e]];
+    TRY(dalloc(&c->d_tempe, tp.size() * sizeof(double)));
+    TRYCU(cudaMemcpy(c->d_tempe, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  std::vector<MatC> mats(c->nmate);
+  for (int im = 0; im < c->nmate; ++im)
+    mats[im] = make_mat(mat->props + 18 * im, mat->e_mart ? mat->e_mart[im] : 0.0, mat->densi[im]);
+  TRY(dalloc(&c->d_mats, mats.size() * sizeof(MatC)));
+  TRYCU(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(MatC), cudaMemcpyHostToDevice));
+
+  // nodal arrays (SoA [3][npad])
+  const size_t nb = 3 * (size_t)c->npad * sizeof(double);
+  double** nodal[] = {&c->d_coord, &c->d_u, &c->d_vt, &c->d_v, &c->d_a, &c->d_f};
+  for (double** p : nodal) {
+    TRY(dalloc(p, nb));
+    TRYCU(cudaMemset(*p, 0, nb));
+  }
+  TRY(dalloc(&c->d_stage, 3 * (size_t)c->npoin * sizeof(double)));
+  TRY(dalloc(&c->d_stage2, 3 * (size_t)c->npoin * sizeof(double)));
+  const unsigned ngrid = (unsigned)ceil_div(c->npoin, 256);
+  TRYCU(cudaMemcpy(c->d_stage, mesh->coord, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyHostToDevice));
+  k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_coord, c->npoin, c->npad);
+  TRYCU(cudaGetLastError());
+
+  // flags, boundary functions, loads
+  std::vector<uint8_t> flags(c->npoin, 0);
+  std::vector<int8_t> bcf(c->npoin, -1);
+  for (int p = 0; p < c->npoin; ++p) {
+    for (int i = 0; i < 3; ++i)
+      if (run->fixno && run->fixno[3 * (int64_t)p + i] == 1) flags[p] |= (uint8_t)(1u << i);
+    if (run->bcfun) bcf[p] = (int8_t)run->bcfun[p];
+  }
+  if (run->fext && run->load_fun >= 0) {
+    c->has_load = true;
+    for (int p = 0; p < c->npoin; ++p)
+      if (run->fext[3 * (int64_t)p] != 0.0 || run->fext[3 * (int64_t)p + 1] != 0.0 ||
+          run->fext[3 * (int64_t)p + 2] != 0.0)
+        flags[p] |= 8u;
+    TRY(dalloc(&c->d_fext, nb));
+    TRYCU(cudaMemset(c->d_fext, 0, nb));
+    TRYCU(cudaMemcpy(c->d_stage, run->fext, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyHostToDevice));
+    k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_fext, c->npoin, c->npad);
+    TRYCU(cudaGetLastError());
+  }
+  TRY(dalloc(&c->d_flags, flags.size()));
+  TRYCU(cudaMemcpy(c->d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice));
+  TRY(dalloc(&c->d_bcfun, bcf.size()));
+  TRYCU(cudaMemcpy(c->d_bcfun, bcf.data(), bcf.size(), cudaMemcpyHostToDevice));
+
+  // lumped mass (constant: geometry and density do not change)
+  c->vmass.assign(c->npoin, 0.0);
+  host_lumped_mass(c->nelem, mesh->lnods, mesh->coord, mesh->lmate, mat->densi, c->vmass);
+  std::vector<double> invm(c->npad, 0.0);
+  for (int p = 0; p < c->npoin; ++p) invm[p] = 1.0 / c->vmass[p];
+  TRY(dalloc(&c->d_invm, invm.size() * sizeof(double)));
+  TRYCU(cudaMemcpy(c->d_invm, invm.data(), invm.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->dtcri = host_critical_dt(c->nelem, mesh->lnods, mesh->coord, mesh->lmate, mat->props,
+                              mat->e_mart, mat->densi);
+
+  // state
+  TRY(c->prec == SMA_PREC_FP32 ? alloc_state<float>(c) : alloc_state<double>(c));
+  TRY(dalloc(&c->d_cnt, NCNT * sizeof(unsigned long long)));
+  TRYCU(cudaMemset(c->d_cnt, 0, NCNT * sizeof(unsigned long long)));
+
+  // time functions and step time
+  FunTab ft;
+  std::memset(&ft, 0, sizeof ft);
+  ft.nfun = nfun;
+  int64_t off = 0;
+  for (int f = 0; f < nfun; ++f) {
+    ft.npts[f] = run->fun_npts[f];
+    ft.smooth[f] = run->fun_smooth ? run->fun_smooth[f] : 0;
+    for (int r = 0; r < ft.npts[f]; ++r)
+      for (int q = 0; q < 4; ++q) ft.tab[f][r][q] = run->fun_tab[off + 4 * r + q];
+    off += 4 * ft.npts[f];
+  }
+  TRY(dalloc(&c->d_ft, sizeof(FunTab)));
+  TRYCU(cudaMemcpy(c->d_ft, &ft, sizeof ft, cudaMemcpyHostToDevice));
+  StepTime ts;
+  std::memset(&ts, 0, sizeof ts);
+  ts.dtime = run->dtime;
+  ts.load_fun = c->has_load ? run->load_fun : -1;
+  TRY(dalloc(&c->d_ts, sizeof(StepTime)));
+  TRYCU(cudaMemcpy(c->d_ts, &ts, sizeof ts, cudaMemcpyHostToDevice));
+  TRYCU(cudaStreamSynchronize(c->stream));
+#undef TRY
+#undef TRYCU
+  *out = c;
+  return SMA_OK;
+}
+
+int32_t sma_explicit_step(sma_ctx* c, int32_t nsteps) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (nsteps < 0) return fail(SMA_ERR_ARG, "nsteps < 0");
+  if (nsteps == 0) return SMA_OK;
+  if (!(c->dtime > 0.0)) return fail(SMA_ERR_STATE, "dtime not set");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc;
+  if (c->nwit > 0) CU(cudaMemsetAsync(c->d_wrow, 0, sizeof(int), c->stream));
+  // prologue: time of step 1 and its predictor from the boundary state
+  k_advance_time<<<1, 1, 0, c->stream>>>(c->d_ts, c->d_ft);
+  c->launches++;
+  if ((rc = launch_nodal(c, 0))) return rc;
+  if (c->timing) {
+    for (int s = 0; s < nsteps; ++s)
+      if ((rc = issue_step_timed(c, s + 1 < nsteps ? 1 : 2))) return rc;
+    return collect_timers(c);
+  }
+  // interior steps (element loop + fused corrector/predictor) as graphs
+  int interior = nsteps - 1;
+  const int chunk = 8;
+  if (interior >= chunk) {
+    if (c->gchunk != chunk && (rc = build_graphs(c, chunk))) return rc;
+    while (interior >= chunk) {
+      CU(cudaGraphLaunch(c->gexec[c->cur], c->stream));
+      c->launches += chunk * kernels_per_step(c);
+      if (chunk & 1) c->cur ^= 1;
+      interior -= chunk;
+    }
+  }
+  for (; interior > 0; --interior)
+    if ((rc = issue_step(c, 1))) return rc;
+  // last step: element loop + corrector only
+  if ((rc = issue_step(c, 2))) return rc;
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_assemble_device(sma_ctx* c, const double* d_displ, double fext_scale, double* d_rhsid) {
+  if (!c || !d_displ || !d_rhsid) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  const unsigned ngrid = (unsigned)ceil_div(c->npoin, 256);
+  k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(d_displ, c->d_u, c->npoin, c->npad);
+  k_fill_f<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin, c->npad);
+  c->launches += 2;
+  CU(cudaGetLastError());
+  int32_t rc = launch_elements(c, false);
+  if (rc) return rc;
+  k_outputs<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin,
+                                          c->npad, d_rhsid, nullptr, nullptr, nullptr);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+int32_t sma_assemble(sma_ctx* c, const double* displ, double fext_scale, double* rhsid,
+                     double* finte, double* fexte, double* frxid, double* vmass) {
+  if (!c || !displ || !rhsid) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  const size_t bytes = 3 * (size_t)c->npoin * sizeof(double);
+  const unsigned ngrid = (unsigned)ceil_div(c->npoin, 256);
+  CU(cudaMemcpyAsync(c->d_stage, displ, bytes, cudaMemcpyHostToDevice, c->stream));
+  k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_u, c->npoin, c->npad);
+  k_fill_f<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin, c->npad);
+  c->launches += 2;
+  CU(cudaGetLastError());
+  int32_t rc = launch_elements(c, false);
+  if (rc) return rc;
+  double* outs[4] = {rhsid, finte, fexte, frxid};
+  for (int q = 0; q < 4; ++q) {
+    if (!outs[q]) continue;
+    double* dr = c->d_stage;
+    k_outputs<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin,
+                                            c->npad, q == 0 ? dr : c->d_stage2,
+                                            q == 1 ? dr : nullptr, q == 2 ? dr : nullptr,
+                                            q == 3 ? dr : nullptr);
+    c->launches++;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(outs[q], dr, bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CU(cudaStreamSynchronize(c->stream));
+  if (vmass) std::memcpy(vmass, c->vmass.data(), c->npoin * sizeof(double));
+  return SMA_OK;
+}
+
+int32_t sma_end_step(sma_ctx* c) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  c->cur ^= 1;
+  return SMA_OK;
+}
+
+int32_t sma_set_nodal(sma_ctx* c, int32_t field, const double* host) {
+  if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
+  double* dst = nullptr;
+  switch (field) {
+    case SMA_FIELD_DISPL: dst = c->d_u; break;
+    case SMA_FIELD_VELOC: dst = c->d_v; break;
+    case SMA_FIELD_ACCEL: dst = c->d_a; break;
+    case SMA_FIELD_RHSID: dst = c->d_f; break;
+    default: return fail(SMA_ERR_ARG, "field not settable");
+  }
+  CU(cudaSetDevice(c->dev));
+  CU(cudaMemcpyAsync(c->d_stage, host, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_aos_to_soa<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(c->d_stage, dst, c->npoin, c->npad);
+  c->launches++;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_get_nodal(sma_ctx* c, int32_t field, double* host) {
+  if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
+  if (field == SMA_FIELD_VMASS) {
+    std::memcpy(host, c->vmass.data(), c->npoin * sizeof(double));
+    return SMA_OK;
+  }
+  const double* src = nullptr;
+  switch (field) {
+    case SMA_FIELD_DISPL: src = c->d_u; break;
+    case SMA_FIELD_VELOC: src = c->d_v; break;
+    case SMA_FIELD_ACCEL: src = c->d_a; break;
+    case SMA_FIELD_RHSID: src = c->d_f; break;
+    default: return fail(SMA_ERR_ARG, "unknown field");
+  }
+  CU(cudaSetDevice(c->dev));
+  k_soa_to_aos<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(src, c->d_stage, c->npoin, c->npad);
+  c->launches++;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(host, c->d_stage, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+static int32_t state_io(sma_ctx* c, double* host, bool in) {
+  if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  const size_t bytes = 48 * (size_t)c->nelem * sizeof(double);
+  double* d = nullptr;
+  int32_t rc = dalloc(&d, bytes);
+  if (rc) return rc;
+  const unsigned grid = (unsigned)ceil_div(8 * (int64_t)c->nelem, 256);
+  // slot ITER_K is the buffer the next element loop writes (cur ^ 1),
+  // slot TIME_N the one it reads (cur)
+  void* sk = c->d_state[c->cur ^ 1];
+  void* sn = c->d_state[c->cur];
+  cudaError_t e = cudaSuccess;
+  if (in) {
+    e = cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+      if (c->prec == SMA_PREC_FP32)
+        k_state_in<float><<<grid, 256, 0, c->stream>>>(d, c->d_perm, (float*)sk, (float*)sn, c->nelem, c->sst);
+      else
+        k_state_in<double><<<grid, 256, 0, c->stream>>>(d, c->d_perm, (double*)sk, (double*)sn, c->nelem, c->sst);
+      e = cudaGetLastError();
+    }
+  } else {
+    if (c->prec == SMA_PREC_FP32)
+      k_state_out<float><<<grid, 256, 0, c->stream>>>(d, c->d_perm, (const float*)sk, (const float*)sn, c->nelem, c->sst);
+    else
+      k_state_out<double><<<grid, 256, 0, c->stream>>>(d, c->d_perm, (const double*)sk, (const double*)sn, c->nelem, c->sst);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, c->stream);
+  }
+  c->launches++;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(SMA_ERR_CUDA, std::string("state I/O: ") + cudaGetErrorString(e));
+  return SMA_OK;
+}
+
+int32_t sma_set_state(sma_ctx* c, const double* host) { return state_io(c, const_cast<double*>(host), true); }
+int32_t sma_get_state(sma_ctx* c, double* host) { return state_io(c, host, false); }
+
+int32_t sma_get_time(sma_ctx* c, double* cutim) {
+  if (!c || !cutim) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  CU(cudaMemcpyAsync(cutim, &c->d_ts->cutim, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_set_time(sma_ctx* c, double cutim) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  CU(cudaMemcpyAsync(&c->d_ts->cutim, &cutim, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_get_counters(sma_ctx* c, sma_counters* out) {
+  if (!c || !out) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  unsigned long long h[NCNT];
+  CU(cudaMemcpyAsync(h, c->d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k < NCNT) ? (int64_t)h[k] : 0;
+  out->gpdet_min = 0.0;
+  return SMA_OK;
+}
+
+int32_t sma_reset_counters(sma_ctx* c) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  CU(cudaMemsetAsync(c->d_cnt, 0, NCNT * sizeof(unsigned long long), c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_set_witness(sma_ctx* c, int32_t nwit, const int32_t* dofs, int32_t max_steps) {
+  if (!c || nwit < 0 || (nwit > 0 && (!dofs || max_steps <= 0))) return fail(SMA_ERR_ARG, "bad witness arguments");
+  for (int w = 0; w < nwit; ++w)
+    if (dofs[w] < 0 || dofs[w] >= 3 * c->npoin) return fail(SMA_ERR_ARG, "witness dof out of range");
+  CU(cudaSetDevice(c->dev));
+  cudaFree(c->d_wdof); cudaFree(c->d_whist); cudaFree(c->d_wrow);
+  c->d_wdof = nullptr; c->d_whist = nullptr; c->d_wrow = nullptr;
+  c->nwit = 0;
+  destroy_graphs(c);
+  if (nwit == 0) return SMA_OK;
+  int32_t rc;
+  if ((rc = dalloc(&c->d_wdof, nwit * sizeof(int32_t)))) return rc;
+  if ((rc = dalloc(&c->d_whist, (size_t)nwit * max_steps * sizeof(double)))) return rc;
+  if ((rc = dalloc(&c->d_wrow, sizeof(int)))) return rc;
+  CU(cudaMemcpy(c->d_wdof, dofs, nwit * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CU(cudaMemset(c->d_wrow, 0, sizeof(int)));
+  c->nwit = nwit;
+  c->wit_max = max_steps;
+  return SMA_OK;
+}
+
+int32_t sma_get_witness(sma_ctx* c, double* host, int32_t* nsteps_out) {
+  if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
+  if (c->nwit <= 0) return fail(SMA_ERR_STATE, "no witnesses set");
+  CU(cudaSetDevice(c->dev));
+  int rows = 0;
+  CU(cudaMemcpy(&rows, c->d_wrow, sizeof(int), cudaMemcpyDeviceToHost));
+  rows = std::min(rows, c->wit_max);
+  CU(cudaMemcpy(host, c->d_whist, (size_t)rows * c->nwit * sizeof(double), cudaMemcpyDeviceToHost));
+  if (nsteps_out) *nsteps_out = rows;
+  return SMA_OK;
+}
+
+int32_t sma_critical_dt(sma_ctx* c, double* dtcri) {
+  if (!c || !dtcri) return fail(SMA_ERR_ARG, "NULL argument");
+  *dtcri = c->dtcri;
+  return SMA_OK;
+}
+
+int32_t sma_set_timing(sma_ctx* c, int32_t enable) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  c->timing = enable != 0;
+  for (int k = 0; k < 3; ++k) { c->tms[k] = 0.0; c->tcnt[k] = 0; }
+  return SMA_OK;
+}
+
+int32_t sma_get_timers(sma_ctx* c, double* ms, int64_t* counts) {
+  if (!c || !ms) return fail(SMA_ERR_ARG, "NULL argument");
+  for (int k = 0; k < 3; ++k) {
+    ms[k] = c->tms[k];
+    if (counts) counts[k] = c->tcnt[k];
+  }
+  return SMA_OK;
+}
+
+void* sma_stream(sma_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int64_t sma_kernel_launches(sma_ctx* c) { return c ? c->launches : 0; }
+
+int32_t sma_eval_law160(int64_t n, const double* props, double e_mart, const double* d_F,
+                        const double* d_tmp, const double* d_sdv_old, double* d_sdv_new,
+                        double* d_pk2, int32_t* d_nr_flag, int32_t precision, void* stream) {
+  if (n < 0) return fail(SMA_ERR_ARG, "n < 0");
+  if (n == 0) return SMA_OK;
+  if (!props || !d_F || !d_sdv_old || !d_sdv_new || !d_pk2) return fail(SMA_ERR_ARG, "NULL argument");
+  if (precision != SMA_PREC_FP64 && precision != SMA_PREC_FP32) return fail(SMA_ERR_ARG, "precision");
+  const MatC m = make_mat(props, e_mart, 1.0);
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned grid = (unsigned)ceil_div(n, 128);
+  if (precision == SMA_PREC_FP32)
+    k_law_batch<float><<<grid, 128, 0, s>>>(n, m, d_F, d_tmp, d_sdv_old, d_sdv_new, d_pk2, d_nr_flag);
+  else
+    k_law_batch<double><<<grid, 128, 0, s>>>(n, m, d_F, d_tmp, d_sdv_old, d_sdv_new, d_pk2, d_nr_flag);
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+}  // extern "C"

@@ -277,6 +277,20 @@ def critical_dt(coord, lnods, props, densi, lmate=None):
     return float(np.min(hmin / c))
 
 
+def prestrain(prob, eps, nu_eff=0.45):
+    """Displacement field of a uniform axial strain eps along x with lateral
+    contraction nu_eff about the cross-section centre, zero on prescribed
+    dofs.  Used to start a timed run on the transformation plateau, where
+    every Gauss point runs the full return map."""
+    X = prob.coord
+    yc = 0.5 * (X[:, 1].min() + X[:, 1].max())
+    zc = 0.5 * (X[:, 2].min() + X[:, 2].max())
+    u = np.stack([eps * (X[:, 0] - X[:, 0].min()), -nu_eff * eps * (X[:, 1] - yc),
+                  -nu_eff * eps * (X[:, 2] - zc)], axis=1)
+    u[prob.fixno == 1] = 0.0
+    return u
+
+
 def _niti_material(ref_equivalent=False):
     props = nitinol_props(**NITI)[None, :]
     e_mart = props[:, 0].copy() if ref_equivalent else np.array([NITI_E_MART])

@@ -1,0 +1,323 @@
+"""Benchmark: Gauss-point updates/s of the explicit SMA (law 160) step.
+
+Workload (one GPU): NiTi cantilever 400x40x40 mm, HEX08 400x40x40 elements
+(640,000 elements, 674,081 nodes, 5.12 M Gauss points), jittered interior
+nodes, clamped root, axial tip traction cycled to 1.5x the forward-finish
+stress; central difference at dt = 0.5 dt_crit.  A step is one pass of the
+explicit scheme over the whole mesh (element loop + nodal update, BCs and
+time advanced on the device).  `value` times the FP32 precision form
+(FP32 kinematics and constitutive update, FP64 return map, force
+accumulation and integration); the plain FP64 form is timed beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp32|fp64] [--scatter atomic|color]
+
+--gpus N > 1 (under torchrun): each rank runs an independent specimen of
+the same workload (the batched-ensemble partition: specimens shard across
+GPUs with no exchange), weak scaling, max over ranks of the device time.
+--impl reference times the CPU restatement of the reference path (the
+oracle: the reference is Fortran and cannot be built here) on the host
+cores of rank 0, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "cantilever_400x40x40_hex08"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--scatter", default="atomic", choices=["atomic", "color"])
+    ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs")
+    ap.add_argument("--div", type=int, default=1, help="coarsen the mesh (tests only)")
+    ap.add_argument("--prestrain", type=float, default=0.01,
+                    help="initial axial strain (both arms): 1%% is just past the AS start")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = []
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]),
+                                 hw=f[5], hwt=f[6], swt=f[7], swp=f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        load = [r for r in rows if r["power"] > 250.0] or rows
+        reasons = sorted({name for r in load for name, key in
+                          (("hw_slowdown", "hw"), ("hw_thermal_slowdown", "hwt"),
+                           ("sw_thermal_slowdown", "swt"), ("sw_power_cap", "swp"))
+                          if r[key].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r["sm"] for r in load),
+                "sm_max_mhz": max(r["smax"] for r in rows), "reasons": reasons,
+                "samples": len(rows), "samples_under_load": len(load)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(precision):
+    """DRAM bytes per element-kernel launch from the committed ncu summary
+    (profiles/k_element_<precision>_cantilever.md, line 'dram_bytes_per_launch: N')."""
+    path = os.path.join(ROOT, "profiles", f"k_element_{precision}_cantilever.md")
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def algorithmic_bytes(prob, precision):
+    """Minimum HBM traffic of one element-kernel launch: connectivity, state
+    read + write, one read of coordinates and displacements and one
+    read-modify-write of the residual per node."""
+    s = 4 if precision == "fp32" else 8
+    return prob.nelem * (32 + 2 * 8 * 3 * s) + prob.npoin * (24 + 24 + 48)
+
+
+def build_problem(div):
+    from alya_sma_b200 import problem as P
+    return P.cantilever_400x40x40(nsteps=20000, div=div)
+
+
+def cpu_baseline(prob, u0, budget_s=15.0, max_steps=50):
+    """The oracle's central-difference step (colour-parallel element loop,
+    OpenMP over all host threads) on the full mesh, as many steps as fit in
+    about budget_s seconds."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    o = O.Problem(prob, nthreads=threads)
+    o.displ[:] = u0
+    o.run(prob.dtime, 1)                      # warm-up (page-in, thread pool)
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        o.run(prob.dtime, 1)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": prob.nelem * 8 * steps / dt, "unit": "GP-updates/s", "cores": threads,
+            "kind": "port", "sample": f"{steps} central-difference steps of the full "
+                                      f"{prob.nelem}-element mesh ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if world > 1 and rank != 0:
+        return 0
+    from alya_sma_b200 import problem as P
+    prob = build_problem(args.div)
+    u0 = P.prestrain(prob, args.prestrain)
+    base = cpu_baseline(prob, u0, budget_s=15.0, max_steps=max(2, args.steps))
+    line = {"impl": "reference", "metric": "Gauss-point updates/s (explicit SMA step)",
+            "value": base["value"], "unit": "GP-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nelem": prob.nelem, "npoin": prob.npoin,
+                       "gauss_points": prob.nelem * 8, "precision": "fp64 (reference CPU path)",
+                       "prestrain": args.prestrain},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "GP-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import alya_sma_b200 as sma
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    prob = build_problem(args.div)
+    nelem, ngp = prob.nelem, prob.nelem * 8
+
+    from alya_sma_b200 import problem as P
+    u0 = P.prestrain(prob, args.prestrain)
+    solid = sma.ExplicitSolid(prob, precision=args.precision, scatter=args.scatter, device=local)
+    solid.set("displ", u0)
+    stream = torch.cuda.ExternalStream(solid.stream)
+    solid.step(max(3, args.warmup))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: K device-resident steps (CUDA graphs) ---------------
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    l0 = solid.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solid.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ck = clocks.stop()
+    launches = solid.kernel_launches - l0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * ngp * args.steps / (ms / 1e3)
+
+    # ---- per-kernel device times (roofline of the element kernel) ---------
+    solid.set_timing(True)
+    solid.step(min(args.steps, 60))
+    tm = solid.timers()
+    solid.set_timing(False)
+    el_ms = tm["element"][0] / max(1, tm["element"][1])
+    nd_ms = tm["nodal"][0] / max(1, tm["nodal"][1])
+    peak, peak_kind = measured_peaks()
+    alg = algorithmic_bytes(prob, args.precision)
+    achieved = alg / (el_ms / 1e3) / 1e9
+    traffic = profiled_traffic(args.precision)
+    roofline = {"bound": "hbm", "kernel": "k_element", "achieved": round(achieved, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg, "launch_ms": round(el_ms, 4),
+                "nodal_launch_ms": round(nd_ms, 4),
+                "note": "compute-bound kernel: the FP32/FP64 pipes, not HBM, bind it"}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        # plain FP64 form on the same mesh
+        if args.precision != "fp64":
+            s64 = sma.ExplicitSolid(prob, precision="fp64", scatter=args.scatter, device=local)
+            s64.set("displ", u0)
+            s64.step(max(3, args.warmup))
+            st64 = torch.cuda.ExternalStream(s64.stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k64 = max(20, args.steps // 4)
+            a.record(st64)
+            s64.step(k64)
+            b.record(st64)
+            b.synchronize()
+            v64 = ngp * k64 / (a.elapsed_time(b) / 1e3)
+            extras["plain_fp64"] = {"value": v64, "unit": "GP-updates/s", "steps": k64}
+            extras["speedup_vs_plain_fp64"] = round(value / world / v64, 3)
+            s64.close()
+        # e2e: the element-loop C-ABI call with pinned host buffers
+        npoin = prob.npoin
+        hd = torch.zeros((npoin, 3), dtype=torch.float64).pin_memory()
+        hr = torch.zeros((npoin, 3), dtype=torch.float64).pin_memory()
+        hd.copy_(torch.from_numpy(solid.get("displ")))
+        dnp, rnp = hd.numpy(), hr.numpy()
+        L = sma.lib()
+        ctx = solid._ctx
+        for _ in range(3):
+            sma._check(L.sma_assemble(ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
+            solid.end_step()
+        ke = max(10, args.steps // 20)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            sma._check(L.sma_assemble(ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
+            solid.end_step()
+        te = time.perf_counter() - t0
+        extras["e2e"] = {"value": ngp * ke / te, "unit": "GP-updates/s",
+                         "h2d_bytes_per_step": 3 * npoin * 8, "d2h_bytes_per_step": 3 * npoin * 8,
+                         "boundary": "sma_assemble (element loop, host displ in, host rhsid out)"}
+        if world == 1:
+            extras["cpu_baseline"] = cpu_baseline(prob, u0)
+    if world > 1:
+        torch.distributed.barrier()
+
+    if rank == 0:
+        line = {"metric": "Gauss-point updates/s (explicit SMA step)", "value": value,
+                "unit": "GP-updates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "fp32" else "f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "nelem": nelem, "npoin": prob.npoin,
+                           "gauss_points": ngp, "precision": args.precision,
+                           "scatter": args.scatter, "dtime": prob.dtime,
+                           "prestrain": args.prestrain,
+                           "l2": "working set > L2 (state, nodal arrays and connectivity "
+                                 f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "roofline": roofline, "gpu_launches": launches, "clocks": ck}
+        line.update(extras)
+        print(json.dumps(line))
+    solid.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

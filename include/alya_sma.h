@@ -1,0 +1,176 @@
+/*
+ * alya_sma.h -- C ABI of the B200 (sm_100a) explicit solid-mechanics step for
+ * superelastic shape-memory alloys (Alya solidz, constitutive law 160).
+ *
+ * Plain pointers, sizes and int32 status codes only, so a Fortran caller binds
+ * it with ISO_C_BINDING (bind(C)) and Python with ctypes.  Every entry point
+ * returns SMA_OK (0) or a negative SMA_ERR_* code; sma_last_error() gives the
+ * message.  Nothing aborts, nothing throws across the boundary.
+ *
+ * Array conventions are the reference's (Fortran column-major):
+ *   lnods  (8, nelem)  int32, 0-based node ids          lnods[a + 8*e]
+ *   coord, displ, veloc, accel, rhsid ... (3, npoin)     x[i + 3*p]
+ *   fixno  (3, npoin)  int32 kfl_fixno_sld codes (1 = prescribed value)
+ *   props  (18, nmate) parco_sld(1:18, imate), order of
+ *          sld_stress_model_160.f90:263-279
+ *   state  (3, 8, 2, nelem) svegm_sld(ielem)%a(1:3,1:8,1:2):
+ *          slot 1 = ITER_K (new), slot 2 = TIME_N (old)
+ *   3x3 tensors: 9 doubles column-major, T(i,j) at [i + 3*j]
+ *
+ * Threading: one host thread per context; calls are ordered on the
+ * context's CUDA stream; a context is not thread-safe.
+ */
+#ifndef ALYA_SMA_H
+#define ALYA_SMA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SMA_OK              0
+#define SMA_ERR_ARG        -1   /* invalid argument or size                  */
+#define SMA_ERR_CUDA       -2   /* CUDA runtime error                         */
+#define SMA_ERR_NOMEM      -3   /* device allocation failed                   */
+#define SMA_ERR_NODEVICE   -4   /* no sm_100 device                           */
+#define SMA_ERR_STATE      -5   /* call out of sequence                       */
+
+/* arithmetic of the element kinematics and the constitutive update */
+#define SMA_PREC_FP64       0   /* all FP64 (the reference's arithmetic)       */
+#define SMA_PREC_FP32       1   /* FP32 kinematics/law, FP64 return map,       */
+                                /* FP64 force accumulation and integration    */
+
+/* scatter-add of element forces into nodal arrays */
+#define SMA_SCATTER_AUTO    0
+#define SMA_SCATTER_ATOMIC  1   /* 8-lane reduce-scatter + FP64 atomics        */
+#define SMA_SCATTER_COLOR   2   /* colour-by-colour plain read-modify-write    */
+                                /* (deterministic; reference sld_elmope.f90:53-99) */
+
+/* nodal fields for sma_set_nodal / sma_get_nodal */
+#define SMA_FIELD_DISPL     0
+#define SMA_FIELD_VELOC     1
+#define SMA_FIELD_ACCEL     2
+#define SMA_FIELD_RHSID     3   /* last assembled residual f_ext - f_int       */
+#define SMA_FIELD_VMASS     4   /* lumped mass, (npoin) only                   */
+
+/* counters (sma_counters.c[k]) accumulated since creation / reset */
+#define SMA_CNT_NR_ACTIVE   0   /* law evaluations with a transformation active */
+#define SMA_CNT_NR_FAILED   1   /* return map hit 65 iterations (state reset)   */
+#define SMA_CNT_NR_BOTH     2   /* AS and SA active together                    */
+#define SMA_CNT_NEG_DET     3   /* Gauss points with det F <= 0                 */
+#define SMA_CNT_NONFINITE   4   /* non-finite nodal accelerations               */
+#define SMA_CNT_FALLBACK64  5   /* FP32 points re-evaluated by the FP64 law     */
+#define SMA_NCOUNTERS       8
+
+typedef struct sma_ctx sma_ctx;
+
+typedef struct {
+  int32_t nelem, npoin;
+  const int32_t* lnods;     /* (8, nelem)                                      */
+  const double*  coord;     /* (3, npoin) reference coordinates                */
+  const int32_t* lmate;     /* (nelem) material ids, or NULL (all material 0)  */
+} sma_mesh_desc;
+
+typedef struct {
+  int32_t nmate;
+  const double* props;      /* (18, nmate)                                     */
+  const double* e_mart;     /* (nmate) martensite modulus (extension) or NULL  */
+  const double* densi;      /* (nmate) density after mass scaling              */
+  const double* tempe;      /* (nelem) temperature (extension) or NULL         */
+} sma_material_desc;
+
+typedef struct {
+  int32_t precision;        /* SMA_PREC_*                                      */
+  int32_t scatter;          /* SMA_SCATTER_*                                   */
+  int32_t device;           /* CUDA device ordinal                             */
+  int32_t nfun;             /* number of DISCRETE time functions (<= 16)       */
+  double  dtime;            /* time step                                       */
+  const int32_t* fixno;     /* (3, npoin) or NULL                              */
+  const int32_t* bcfun;     /* (npoin) time function of the fixed dofs or -1   */
+  const int32_t* fun_npts;  /* (nfun) rows per table (<= 32)                   */
+  const int32_t* fun_smooth;/* (nfun) 1 = SMOOTH step, 0 = linear              */
+  const double*  fun_tab;   /* concatenated (4, npts) tables (t, vx, vy, vz)   */
+  const double*  fext;      /* (3, npoin) nodal load at load factor 1, or NULL */
+  int32_t load_fun;         /* table whose vx column scales fext, or -1        */
+  int32_t block;            /* threads per element-kernel block (0 = tuned)    */
+} sma_run_desc;
+
+typedef struct { int64_t c[SMA_NCOUNTERS]; double gpdet_min; } sma_counters;
+
+/* Context: copies the host arrays to the device and owns every device buffer.
+ * Replaces the reference's Begrun-time set-up of solidz (sld_inivar, mass) */
+int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
+                       const sma_run_desc* run, sma_ctx** out);
+int32_t sma_ctx_destroy(sma_ctx* ctx);
+
+/* Step boundary: nsteps explicit central-difference steps, device resident,
+ * replayed as CUDA graphs.  Replaces one pass of Timste/Begste/sld_explicit/
+ * Endste per step (mod_sld_solution_methods.f90:101-223,
+ * sld_updbcs.f90:85-114, sld_updunk.f90:149-185). */
+int32_t sma_explicit_step(sma_ctx* ctx, int32_t nsteps);
+
+/* Element-loop boundary with HOST buffers: displ (3,npoin) in; rhsid, finte,
+ * fexte, frxid (3,npoin) and vmass (npoin) out (any output may be NULL
+ * except rhsid).  Reads state slot TIME_N, writes slot ITER_K.  Replaces
+ * sld_matrix(SLD_EXPLICIT_SCHEME) -> sld_elmope (sld_matrix.f90:161-171). */
+int32_t sma_assemble(sma_ctx* ctx, const double* displ, double fext_scale,
+                     double* rhsid, double* finte, double* fexte, double* frxid,
+                     double* vmass);
+/* same with device pointers (no host copies), ordered on the context stream */
+int32_t sma_assemble_device(sma_ctx* ctx, const double* d_displ, double fext_scale,
+                            double* d_rhsid);
+/* sld_updunk(ITASK_ENDSTE) for the state: slot TIME_N <- slot ITER_K */
+int32_t sma_end_step(sma_ctx* ctx);
+
+/* Material-plugin boundary, batched: n independent Gauss points with device
+ * pointers F (9n), tmp (n or NULL), sdv_old/sdv_new (3n), pk2 (9n),
+ * nr_flag (n or NULL).  Replaces eval_sld_stress_model_160 with flagt = 0
+ * (sld_stress_model_160.f90:36-195).  precision: SMA_PREC_*.
+ * stream: a cudaStream_t or NULL for the default stream. */
+int32_t sma_eval_law160(int64_t n, const double* props, double e_mart,
+                        const double* d_F, const double* d_tmp,
+                        const double* d_sdv_old, double* d_sdv_new, double* d_pk2,
+                        int32_t* d_nr_flag, int32_t precision, void* stream);
+
+/* host <-> context data */
+int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);
+int32_t sma_get_nodal(sma_ctx* ctx, int32_t field, double* host);
+int32_t sma_set_state(sma_ctx* ctx, const double* host_sdv);   /* (3,8,2,nelem) */
+int32_t sma_get_state(sma_ctx* ctx, double* host_sdv);
+int32_t sma_get_time(sma_ctx* ctx, double* cutim);
+int32_t sma_set_time(sma_ctx* ctx, double cutim);
+int32_t sma_get_counters(sma_ctx* ctx, sma_counters* out);
+int32_t sma_reset_counters(sma_ctx* ctx);
+/* witness dofs (flat ids 3*p+i): their displacement after each step of the
+ * next sma_explicit_step call is recorded on the device; sma_get_witness
+ * copies (nsteps, nwit) values of the last call. */
+int32_t sma_set_witness(sma_ctx* ctx, int32_t nwit, const int32_t* dofs, int32_t max_steps);
+int32_t sma_get_witness(sma_ctx* ctx, double* host, int32_t* nsteps_out);
+
+/* critical time step of the mesh (mod_sld_minle_time_step.f90:262-268) */
+int32_t sma_critical_dt(sma_ctx* ctx, double* dtcri);
+
+/* the CUDA stream of the context (cudaStream_t) for callers that overlap */
+void* sma_stream(sma_ctx* ctx);
+
+/* Per-phase device timers (the reference's times(k)%ini/%add brackets,
+ * sld_element_operations.f90:125-266 and sld_matrix.f90:159-173): while
+ * enabled, sma_explicit_step launches kernels directly (no graph) with CUDA
+ * events around each phase.  ms[0] element loop, ms[1] nodal update,
+ * ms[2] whole steps; counts[] the launches timed in each. */
+#define SMA_NTIMERS 3
+int32_t sma_set_timing(sma_ctx* ctx, int32_t enable);
+int32_t sma_get_timers(sma_ctx* ctx, double* ms, int64_t* counts);
+
+/* kernel launches issued by this context since creation (all kernels) */
+int64_t sma_kernel_launches(sma_ctx* ctx);
+
+const char* sma_last_error(void);
+const char* sma_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
