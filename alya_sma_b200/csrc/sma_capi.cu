@@ -346,9 +346,9 @@ int32_t issue_step(sma_ctx* c, int nodal_mode) {
   int32_t rc = launch_elements(c, true);
   if (rc) return rc;
   c->cur ^= 1;   // the state written by this step is TIME_N of the next
-  rc = launch_nodal(c, nodal_mode);
-  if (rc) return rc;
-  return launch_witness(c);
+  // u holds u_k until the nodal kernel predicts u_{k+1}
+  if ((rc = launch_witness(c))) return rc;
+  return launch_nodal(c, nodal_mode);
 }
 
 int32_t next_event(sma_ctx* c, int* idx) {
@@ -370,12 +370,13 @@ int32_t issue_step_timed(sma_ctx* c, int nodal_mode) {
   if ((rc = launch_elements(c, true))) return rc;
   c->cur ^= 1;
   if ((rc = next_event(c, &e1))) return rc;
+  if ((rc = launch_witness(c))) return rc;
   if ((rc = launch_nodal(c, nodal_mode))) return rc;
   if ((rc = next_event(c, &e2))) return rc;
   c->evmarks.push_back({0, {e0, e1}});
   c->evmarks.push_back({1, {e1, e2}});
   c->evmarks.push_back({2, {e0, e2}});
-  return launch_witness(c);
+  return SMA_OK;
 }
 
 int32_t collect_timers(sma_ctx* c) {
@@ -936,3 +937,4 @@ int32_t sma_eval_law160(int64_t n, const double* props, double e_mart, const dou
 }
 
 }  // extern "C"
+
