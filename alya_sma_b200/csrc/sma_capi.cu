@@ -938,3 +938,144 @@ int32_t sma_eval_law160(int64_t n, const double* props, double e_mart, const dou
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// Element loop that allocates nothing.
+//
+// For callers that must not (or cannot) allocate device memory through the
+// CUDA runtime: a Fortran host whose device arrays are owned by an OpenACC
+// data region or a caller-side memory pool, or code running where a
+// cudaMalloc would synchronise the device or break a caller's allocation
+// budget.  The caller passes every input and output as a device pointer; the
+// working set the element kernel needs beyond them (structure-of-arrays
+// copies of coordinates and displacements, the FP64 force accumulator, the
+// state in the kernel's layout, the material constants and the counters)
+// lives in one file-scope device array of fixed size, reserved when the
+// library is loaded and held by every GPU that loads it until the process
+// exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t NA_NPAD = SMA_NOALLOC_MAX_NODES;          // multiple of 32
+constexpr int64_t NA_SST = 8 * (int64_t)SMA_NOALLOC_MAX_ELEMS;
+constexpr size_t NA_NODAL = 3 * (size_t)NA_NPAD * sizeof(double);
+constexpr size_t NA_STATE = 3 * (size_t)NA_SST * sizeof(double);
+constexpr size_t NA_OFF_COORD = 0;
+constexpr size_t NA_OFF_U = NA_OFF_COORD + NA_NODAL;
+constexpr size_t NA_OFF_F = NA_OFF_U + NA_NODAL;
+constexpr size_t NA_OFF_S0 = NA_OFF_F + NA_NODAL;
+constexpr size_t NA_OFF_S1 = NA_OFF_S0 + NA_STATE;
+constexpr size_t NA_OFF_MAT = NA_OFF_S1 + NA_STATE;
+constexpr size_t NA_OFF_CNT = NA_OFF_MAT + 256;
+constexpr size_t NA_OFF_FLAG = NA_OFF_CNT + 256;
+constexpr size_t NA_BYTES = NA_OFF_FLAG + 256;
+static_assert(NA_NPAD % 32 == 0, "node capacity must be a multiple of 32");
+static_assert(sizeof(MatC) <= 256, "material block");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+// device address of g_noalloc_scratch per device ordinal (host code cannot
+// use the symbol's name as an address)
+unsigned char* g_noalloc_ptr[64] = {nullptr};
+
+__global__ void k_put_mat(MatC m, MatC* dst) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = m;
+}
+
+// flag = 1 if any node id of lnods lies outside [0, npoin)
+__global__ void k_check_lnods(const int32_t* lnods, int64_t n, int32_t npoin, int32_t* flag) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    const int32_t v = lnods[k];
+    if (v < 0 || v >= npoin) atomicOr(flag, 1);
+  }
+}
+
+template <typename T>
+int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int32_t* d_lnods,
+                    double* d_sdv, cudaStream_t s) {
+  const int64_t sst = ceil_div(8 * (int64_t)nelem, 32) * 32;
+  T* s_iterk = (T*)(base + NA_OFF_S0);
+  T* s_timen = (T*)(base + NA_OFF_S1);
+  const unsigned sgrid = (unsigned)ceil_div(8 * (int64_t)nelem, 256);
+  k_state_in<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
+  ElemArgs<T> a;
+  std::memset(&a, 0, sizeof a);
+  a.lnods = d_lnods;
+  a.coord = (const double*)(base + NA_OFF_COORD);
+  a.u = (const double*)(base + NA_OFF_U);
+  a.f = (double*)(base + NA_OFF_F);
+  a.lmate = nullptr;
+  a.mats = (const MatC*)(base + NA_OFF_MAT);
+  a.tempe = nullptr;
+  a.sold = s_timen;
+  a.snew = s_iterk;
+  a.cnt = (unsigned long long*)(base + NA_OFF_CNT);
+  a.ts = nullptr;
+  a.ft = nullptr;
+  a.npad = NA_NPAD;
+  a.sst = sst;
+  a.beg = 0;
+  a.end = nelem;
+  a.has_grav = 0;
+  const int block = 256, epb = block / 8;
+  const size_t smem = (size_t)epb * 9 * sizeof(ElemSmem<T>);
+  k_element<T, true><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
+  k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int32_t* d_lnods,
+                                        const double* d_coord, const double* d_displ,
+                                        const double* props, double e_mart, double* d_sdv,
+                                        double* d_rhsid, int32_t precision, void* stream) {
+  if (nelem <= 0 || npoin <= 0) return fail(SMA_ERR_ARG, "nelem and npoin must be positive");
+  if (npoin > SMA_NOALLOC_MAX_NODES || nelem > SMA_NOALLOC_MAX_ELEMS)
+    return fail(SMA_ERR_ARG, "sma_assemble_noalloc: mesh of " + std::to_string(nelem) + " elements, " +
+                                 std::to_string(npoin) + " nodes exceeds the fixed scratch capacity of " +
+                                 std::to_string(SMA_NOALLOC_MAX_ELEMS) + " elements and " +
+                                 std::to_string(SMA_NOALLOC_MAX_NODES) + " nodes");
+  if (!d_lnods || !d_coord || !d_displ || !props || !d_sdv || !d_rhsid)
+    return fail(SMA_ERR_ARG, "NULL argument");
+  if (precision != SMA_PREC_FP64 && precision != SMA_PREC_FP32) return fail(SMA_ERR_ARG, "precision");
+  if (!(props[0] > 0.0) || !(props[1] > -1.0 && props[1] < 0.5))
+    return fail(SMA_ERR_ARG, "material: need E > 0, -1 < nu < 0.5");
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SMA_ERR_ARG, "device ordinal beyond 63");
+  if (!g_noalloc_ptr[dev]) {
+    // set-up, once per device, with that device current
+    void* p = nullptr;
+    CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  // reject node ids outside [0, npoin) before any kernel dereferences them
+  int32_t* d_flag = (int32_t*)(base + NA_OFF_FLAG);
+  CU(cudaMemsetAsync(d_flag, 0, sizeof(int32_t), s));
+  k_check_lnods<<<(unsigned)ceil_div(8 * (int64_t)nelem, 256), 256, 0, s>>>(d_lnods, 8 * (int64_t)nelem,
+                                                                           npoin, d_flag);
+  CU(cudaGetLastError());
+  int32_t bad = 0;
+  CU(cudaMemcpyAsync(&bad, d_flag, sizeof bad, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (bad) return fail(SMA_ERR_ARG, "lnods holds node ids outside [0, npoin)");
+  // the scratch keeps the previous call's contents: clear what accumulates
+  CU(cudaMemsetAsync(base + NA_OFF_F, 0, NA_NODAL, s));
+  CU(cudaMemsetAsync(base + NA_OFF_CNT, 0, 256, s));
+  const unsigned ngrid = (unsigned)ceil_div(npoin, 256);
+  k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_coord, (double*)(base + NA_OFF_COORD), npoin, NA_NPAD);
+  k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_displ, (double*)(base + NA_OFF_U), npoin, NA_NPAD);
+  k_put_mat<<<1, 1, 0, s>>>(make_mat(props, e_mart, 1.0), (MatC*)(base + NA_OFF_MAT));
+  CU(cudaGetLastError());
+  int32_t rc = (precision == SMA_PREC_FP32)
+                   ? noalloc_run<float>(base, nelem, npoin, d_lnods, d_sdv, s)
+                   : noalloc_run<double>(base, nelem, npoin, d_lnods, d_sdv, s);
+  if (rc) return rc;
+  k_soa_to_aos<<<ngrid, 256, 0, s>>>((const double*)(base + NA_OFF_F), d_rhsid, npoin, NA_NPAD);
+  CU(cudaGetLastError());
+  return SMA_OK;
+}

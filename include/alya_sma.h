@@ -134,6 +134,31 @@ int32_t sma_eval_law160(int64_t n, const double* props, double e_mart,
                         const double* d_sdv_old, double* d_sdv_new, double* d_pk2,
                         int32_t* d_nr_flag, int32_t precision, void* stream);
 
+/* Element loop that allocates nothing.  No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory themselves
+ * through the CUDA runtime (a Fortran host whose device arrays belong to an
+ * OpenACC data region or a caller-side pool, code where a cudaMalloc would
+ * synchronise the device or exceed the caller's memory budget).  Inputs and
+ * outputs are caller-owned device pointers: lnods (8,nelem) with node ids in
+ * [0,npoin), coord and displ (3,npoin), sdv (3,8,2,nelem) read at slot
+ * TIME_N and written at slot ITER_K, rhsid (3,npoin) = f_ext - f_int of the
+ * element loop (no nodal loads); props is a host array of 18 doubles.
+ * The working set lives in one fixed device array compiled into the
+ * library (about 7.5 MB, held by every GPU that loads the library until the
+ * process exits), so meshes are limited to SMA_NOALLOC_MAX_ELEMS elements and
+ * SMA_NOALLOC_MAX_NODES nodes; larger ones return SMA_ERR_ARG.  The first
+ * call on a device looks up that array's device address (make it before any
+ * stream capture on that device); every call validates lnods with one host
+ * synchronisation.  All calls share the array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the
+ * caller.  Ordered on `stream` (NULL: default stream). */
+#define SMA_NOALLOC_MAX_NODES 16384
+#define SMA_NOALLOC_MAX_ELEMS 16384
+int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int32_t* d_lnods,
+                             const double* d_coord, const double* d_displ,
+                             const double* props, double e_mart, double* d_sdv,
+                             double* d_rhsid, int32_t precision, void* stream);
+
 /* host <-> context data */
 int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);
 int32_t sma_get_nodal(sma_ctx* ctx, int32_t field, double* host);
