@@ -54,7 +54,12 @@ class _Run(C.Structure):
                 ("nfun", C.c_int32), ("dtime", C.c_double), ("fixno", C.c_void_p),
                 ("bcfun", C.c_void_p), ("fun_npts", C.c_void_p), ("fun_smooth", C.c_void_p),
                 ("fun_tab", C.c_void_p), ("fext", C.c_void_p), ("load_fun", C.c_int32),
-                ("block", C.c_int32)]
+                ("block", C.c_int32), ("scheme", C.c_int32), ("phitw", C.c_double),
+                ("variant", C.c_int32)]
+
+
+SCHEME = {"cd": 0, "tw": 1}
+VARIANT = {"auto": 0, "pipe": 1, "plain": 2}
 
 
 class _Counters(C.Structure):
@@ -105,6 +110,10 @@ def lib():
         L.sma_critical_dt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.sma_set_timing.argtypes = [C.c_void_p, C.c_int32]
         L.sma_get_timers.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.sma_set_energy.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        L.sma_get_energy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]
+        L.sma_checkpoint_save.argtypes = [C.c_void_p, C.c_char_p]
+        L.sma_checkpoint_load.argtypes = [C.c_void_p, C.c_char_p]
         _lib = L
     return _lib
 
@@ -130,7 +139,8 @@ class ExplicitSolid:
     constitutive update in FP32 (return map, force accumulation and time
     integration stay FP64)."""
 
-    def __init__(self, prob, precision="fp64", scatter="atomic", device=0, dtime=None, block=0):
+    def __init__(self, prob, precision="fp64", scatter="atomic", device=0, dtime=None, block=0,
+                 scheme="cd", phitw=0.0, variant="auto"):
         L = lib()
         self.prob = prob
         self.precision = precision
@@ -150,7 +160,7 @@ class ExplicitSolid:
         run = _Run(PREC[precision], SCATTER[scatter], device, int(k["fun_npts"].size),
                    float(prob.dtime if dtime is None else dtime), _p(k["fixno"]), _p(k["bcfun"]),
                    _p(k["fun_npts"]), _p(k["fun_smooth"]), _p(k["fun_tab"]), _p(k["fext"]),
-                   int(prob.load_fun), int(block))
+                   int(prob.load_fun), int(block), SCHEME[scheme], float(phitw), VARIANT[variant])
         self._ctx = C.c_void_p()
         _check(L.sma_ctx_create(C.byref(mesh), C.byref(mat), C.byref(run), C.byref(self._ctx)))
 
@@ -244,6 +254,28 @@ class ExplicitSolid:
         d = C.c_double()
         _check(lib().sma_critical_dt(self._ctx, C.byref(d)))
         return d.value
+
+    def set_energy(self, on=True, max_steps=0):
+        """Energy balance of sld_energy after every step (history rows of
+        ALLIE, ALLWK, ALLKE, ETOTA, EENER up to max_steps)."""
+        _check(lib().sma_set_energy(self._ctx, int(bool(on)), int(max_steps)))
+        self._emax = int(max_steps)
+
+    def energy(self):
+        """(totals dict, history array (nrows, 5))."""
+        tot = np.zeros(5)
+        hist = np.zeros((max(1, getattr(self, "_emax", 0)), 5))
+        n = C.c_int32()
+        _check(lib().sma_get_energy(self._ctx, _p(tot), _p(hist), C.byref(n)))
+        names = ("allie", "allwk", "allke", "etota", "eener")
+        return {k: float(tot[i]) for i, k in enumerate(names)}, hist[: n.value]
+
+    def save(self, path):
+        """Checkpoint of the step-boundary state (restart)."""
+        _check(lib().sma_checkpoint_save(self._ctx, os.fsencode(path)))
+
+    def load(self, path):
+        _check(lib().sma_checkpoint_load(self._ctx, os.fsencode(path)))
 
     def set_timing(self, on=True):
         _check(lib().sma_set_timing(self._ctx, int(bool(on))))

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -180,6 +181,10 @@ MatC make_mat(const double* pr, double e_mart, double densi) {
   m.EA = E;
   m.EM = (e_mart > 0.0) ? e_mart : E;
   m.nu = v;
+  m.iEA = 1.0 / m.EA;
+  m.iEM = 1.0 / m.EM;
+  m.kK = 1.0 / (3.0 - 6.0 * v);
+  m.kG = 1.0 / (2.0 + 2.0 * v);
   m.densi = densi;
   m.ext_E = (e_mart > 0.0 && e_mart != E) ? 1 : 0;
   return m;
@@ -196,6 +201,9 @@ struct sma_ctx {
   int prec = SMA_PREC_FP64;
   int scatter = SMA_SCATTER_ATOMIC;
   int block = 256;
+  int variant = SMA_VARIANT_PIPE;
+  int nsm = 148;                           // multiprocessors of the device
+  int resident = 0;                        // resident pipelined blocks per SM (lazy)
   int nelem = 0, npoin = 0;
   int64_t npad = 0, sst = 0;
   int nmate = 0;
@@ -219,6 +227,7 @@ struct sma_ctx {
   uint8_t* d_flags = nullptr;
   int8_t* d_bcfun = nullptr;
   MatC* d_mats = nullptr;
+  MatC mat0;                               // material 0, passed by value when nmate == 1
   void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
   int cur = 0;                             // state buffer holding TIME_N
   unsigned long long* d_cnt = nullptr;
@@ -231,6 +240,17 @@ struct sma_ctx {
   int32_t* d_wdof = nullptr;
   double* d_whist = nullptr;
   int* d_wrow = nullptr;
+  // scheme and energy balance
+  int scheme = SMA_SCHEME_CD;
+  bool energy = false;
+  int ehist_max = 0;
+  double* d_uprev = nullptr;
+  double* d_fintp = nullptr;
+  double* d_fextp = nullptr;
+  double* d_en = nullptr;                  // [4..8] totals (ALLIE, ALLWK, ALLKE, EENER, steps)
+  double* d_epart = nullptr;               // per-block partial sums of the nodal kernel
+  double* d_ehist = nullptr;
+  int* d_erow = nullptr;
   // host copies
   std::vector<double> vmass;
   double dtcri = 0.0;
@@ -271,6 +291,7 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance) {
   a.sst = c->sst;
   a.beg = beg;
   a.end = end;
+  a.mat0 = c->mat0;
   a.grav[0] = c->grav[0];
   a.grav[1] = c->grav[1];
   a.grav[2] = c->grav[2];
@@ -278,20 +299,48 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance) {
   return a;
 }
 
+// resident blocks per SM of a kernel at this block size and shared memory
+template <typename K>
+int32_t resident_blocks(K kernel, int block, size_t smem, int* out) {
+  CU(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, kernel, block, smem));
+  if (*out < 1) return fail(SMA_ERR_ARG, "element kernel does not fit on an SM at this block size");
+  return SMA_OK;
+}
+
+// kernel attributes and the persistent grid, fixed at context creation (not
+// inside a stream capture)
+template <typename T>
+int32_t init_element_launch_t(sma_ctx* c) {
+  if (c->variant != SMA_VARIANT_PIPE) return SMA_OK;
+  const size_t smem = element_pipe_smem_bytes<T>(c->block);
+  return (c->scatter == SMA_SCATTER_COLOR)
+             ? resident_blocks(k_element_pipe<T, false>, c->block, smem, &c->resident)
+             : resident_blocks(k_element_pipe<T, true>, c->block, smem, &c->resident);
+}
+
 template <typename T>
 int32_t launch_elements_t(sma_ctx* c, bool advance) {
   const int nrange = (int)c->cptr.size() - 1;
   const int epb = c->block / 8;
-  const size_t smem = (size_t)epb * 9 * sizeof(ElemSmem<T>);
+  const bool color = c->scatter == SMA_SCATTER_COLOR;
+  if (c->variant == SMA_VARIANT_PIPE && c->resident == 0)
+    return fail(SMA_ERR_STATE, "element launch not initialised");
   for (int r = 0; r < nrange; ++r) {
     const int beg = c->cptr[r], end = c->cptr[r + 1];
     if (end <= beg) continue;
     ElemArgs<T> a = elem_args<T>(c, beg, end, advance && r == 0);
-    const unsigned grid = (unsigned)ceil_div(end - beg, epb);
-    if (c->scatter == SMA_SCATTER_COLOR)
-      k_element<T, false><<<grid, c->block, smem, c->stream>>>(a);
-    else
-      k_element<T, true><<<grid, c->block, smem, c->stream>>>(a);
+    const int64_t ntiles = ceil_div(end - beg, epb);
+    if (c->variant == SMA_VARIANT_PIPE) {
+      const size_t smem = element_pipe_smem_bytes<T>(c->block);
+      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident);
+      if (color) k_element_pipe<T, false><<<grid, c->block, smem, c->stream>>>(a);
+      else k_element_pipe<T, true><<<grid, c->block, smem, c->stream>>>(a);
+    } else {
+      const size_t smem = element_smem_bytes<T>(c->block);
+      if (color) k_element<T, false><<<(unsigned)ntiles, c->block, smem, c->stream>>>(a);
+      else k_element<T, true><<<(unsigned)ntiles, c->block, smem, c->stream>>>(a);
+    }
     c->launches++;
   }
   CU(cudaGetLastError());
@@ -316,26 +365,49 @@ NodalArgs nodal_args(sma_ctx* c) {
   a.fext = c->d_fext;
   a.ts = c->d_ts;
   a.cnt = c->d_cnt;
+  a.uprev = c->d_uprev;
+  a.fint_prev = c->d_fintp;
+  a.fext_prev = c->d_fextp;
+  a.en_step = c->d_epart;
   a.npoin = c->npoin;
   a.npad = c->npad;
   return a;
 }
 
+template <int MODE>
+void launch_nodal_mode(sma_ctx* c, unsigned grid, const NodalArgs& a) {
+  const bool en = c->energy && MODE >= 1;
+  if (c->scheme == SMA_SCHEME_TW) {
+    if (en) k_nodal<MODE, SCHEME_TW, true><<<grid, 256, 0, c->stream>>>(a);
+    else k_nodal<MODE, SCHEME_TW, false><<<grid, 256, 0, c->stream>>>(a);
+  } else {
+    if (en) k_nodal<MODE, SCHEME_CD, true><<<grid, 256, 0, c->stream>>>(a);
+    else k_nodal<MODE, SCHEME_CD, false><<<grid, 256, 0, c->stream>>>(a);
+  }
+}
+
 int32_t launch_nodal(sma_ctx* c, int mode) {
   const unsigned grid = (unsigned)ceil_div(c->npoin, 256);
   NodalArgs a = nodal_args(c);
-  if (mode == 0) k_nodal<0><<<grid, 256, 0, c->stream>>>(a);
-  else if (mode == 1) k_nodal<1><<<grid, 256, 0, c->stream>>>(a);
-  else k_nodal<2><<<grid, 256, 0, c->stream>>>(a);
+  if (mode == 0) launch_nodal_mode<0>(c, grid, a);
+  else if (mode == 1) launch_nodal_mode<1>(c, grid, a);
+  else launch_nodal_mode<2>(c, grid, a);
   c->launches++;
   CU(cudaGetLastError());
+  if (c->energy && mode >= 1) {
+    k_energy_finalize<<<1, 256, 0, c->stream>>>(c->d_epart, (int)ceil_div(c->npoin, 256), c->d_en + 4,
+                                                 c->d_ehist, c->d_erow,
+                                               c->ehist_max);
+    c->launches++;
+    CU(cudaGetLastError());
+  }
   return SMA_OK;
 }
 
 int32_t launch_witness(sma_ctx* c) {
   if (c->nwit <= 0) return SMA_OK;
-  k_witness<<<1, 128, 0, c->stream>>>(c->d_u, c->npad, c->d_wdof, c->nwit, c->d_whist,
-                                      c->d_wrow, c->wit_max);
+  k_witness<<<1, 128, 0, c->stream>>>(c->d_u, c->d_f, c->npoin, c->npad, c->d_wdof, c->nwit,
+                                      c->d_whist, c->d_wrow, c->wit_max);
   c->launches++;
   CU(cudaGetLastError());
   return SMA_OK;
@@ -426,7 +498,7 @@ int32_t build_graphs(sma_ctx* c, int chunk) {
 }
 
 int64_t kernels_per_step(const sma_ctx* c) {
-  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0);
+  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0);
 }
 
 template <typename T>
@@ -455,7 +527,8 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
   void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_coord, c->d_u, c->d_vt, c->d_v, c->d_a,
                   c->d_f, c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
-                  c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow};
+                  c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
+                  c->d_fextp, c->d_en, c->d_ehist, c->d_erow, c->d_epart};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -476,6 +549,8 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   if (run->nfun < 0 || run->nfun > MAXFUN) return fail(SMA_ERR_ARG, "at most 16 time functions");
   if (run->block != 0 && (run->block % 32 != 0 || run->block < 32 || run->block > 256))
     return fail(SMA_ERR_ARG, "block must be a multiple of 32 in [32, 256]");
+  if (run->scheme != SMA_SCHEME_CD && run->scheme != SMA_SCHEME_TW)
+    return fail(SMA_ERR_ARG, "scheme must be SMA_SCHEME_CD or SMA_SCHEME_TW");
   for (int64_t k = 0; k < 8 * (int64_t)mesh->nelem; ++k)
     if (mesh->lnods[k] < 0 || mesh->lnods[k] >= mesh->npoin)
       return fail(SMA_ERR_ARG, "lnods entry out of range at " + std::to_string(k));
@@ -529,13 +604,22 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   TRYCU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   c->prec = run->precision;
   c->scatter = (run->scatter == SMA_SCATTER_COLOR) ? SMA_SCATTER_COLOR : SMA_SCATTER_ATOMIC;
-  c->block = run->block ? run->block : 256;
+  // defaults measured on B200 (cantilever 640k elements, blocks 64..256):
+  // FP32 pipelined 256 threads; FP64 plain 128 threads (the pipelined FP64
+  // kernel needs ~200 registers and loses occupancy)
+  if (run->variant == SMA_VARIANT_AUTO)
+    c->variant = (c->prec == SMA_PREC_FP32) ? SMA_VARIANT_PIPE : SMA_VARIANT_PLAIN;
+  else
+    c->variant = (run->variant == SMA_VARIANT_PLAIN) ? SMA_VARIANT_PLAIN : SMA_VARIANT_PIPE;
+  c->block = run->block ? run->block : ((c->variant == SMA_VARIANT_PIPE) ? 256 : 128);
+  c->nsm = prop.multiProcessorCount;
   c->nelem = mesh->nelem;
   c->npoin = mesh->npoin;
   c->npad = ceil_div(c->npoin, 32) * 32;
   c->sst = ceil_div(8 * (int64_t)c->nelem, 32) * 32;
   c->nmate = mat->nmate;
   c->dtime = run->dtime;
+  c->scheme = run->scheme;
 
   // element order
   c->perm.resize(c->nelem);
@@ -570,6 +654,7 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
     mats[im] = make_mat(mat->props + 18 * im, mat->e_mart ? mat->e_mart[im] : 0.0, mat->densi[im]);
   TRY(dalloc(&c->d_mats, mats.size() * sizeof(MatC)));
   TRYCU(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(MatC), cudaMemcpyHostToDevice));
+  c->mat0 = mats[0];
 
   // nodal arrays (SoA [3][npad])
   const size_t nb = 3 * (size_t)c->npad * sizeof(double);
@@ -622,6 +707,7 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
 
   // state
   TRY(c->prec == SMA_PREC_FP32 ? alloc_state<float>(c) : alloc_state<double>(c));
+  TRY(c->prec == SMA_PREC_FP32 ? init_element_launch_t<float>(c) : init_element_launch_t<double>(c));
   TRY(dalloc(&c->d_cnt, NCNT * sizeof(unsigned long long)));
   TRYCU(cudaMemset(c->d_cnt, 0, NCNT * sizeof(unsigned long long)));
 
@@ -643,6 +729,7 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   std::memset(&ts, 0, sizeof ts);
   ts.dtime = run->dtime;
   ts.load_fun = c->has_load ? run->load_fun : -1;
+  ts.phi = (run->phitw != 0.0) ? run->phitw : 1.033;   // sld_reanut.f90:176 default
   TRY(dalloc(&c->d_ts, sizeof(StepTime)));
   TRYCU(cudaMemcpy(c->d_ts, &ts, sizeof ts, cudaMemcpyHostToDevice));
   TRYCU(cudaStreamSynchronize(c->stream));
@@ -862,7 +949,7 @@ int32_t sma_reset_counters(sma_ctx* c) {
 int32_t sma_set_witness(sma_ctx* c, int32_t nwit, const int32_t* dofs, int32_t max_steps) {
   if (!c || nwit < 0 || (nwit > 0 && (!dofs || max_steps <= 0))) return fail(SMA_ERR_ARG, "bad witness arguments");
   for (int w = 0; w < nwit; ++w)
-    if (dofs[w] < 0 || dofs[w] >= 3 * c->npoin) return fail(SMA_ERR_ARG, "witness dof out of range");
+    if (dofs[w] < 0 || dofs[w] >= 6 * c->npoin) return fail(SMA_ERR_ARG, "witness id out of range");
   CU(cudaSetDevice(c->dev));
   cudaFree(c->d_wdof); cudaFree(c->d_whist); cudaFree(c->d_wrow);
   c->d_wdof = nullptr; c->d_whist = nullptr; c->d_wrow = nullptr;
@@ -890,6 +977,156 @@ int32_t sma_get_witness(sma_ctx* c, double* host, int32_t* nsteps_out) {
   CU(cudaMemcpy(host, c->d_whist, (size_t)rows * c->nwit * sizeof(double), cudaMemcpyDeviceToHost));
   if (nsteps_out) *nsteps_out = rows;
   return SMA_OK;
+}
+
+int32_t sma_set_energy(sma_ctx* c, int32_t enable, int32_t max_steps) {
+  if (!c || (enable && max_steps < 0)) return fail(SMA_ERR_ARG, "bad energy arguments");
+  CU(cudaSetDevice(c->dev));
+  destroy_graphs(c);
+  c->energy = false;
+  if (!enable) return SMA_OK;
+  const size_t nb = 3 * (size_t)c->npad * sizeof(double);
+  int32_t rc;
+  if (!c->d_uprev) {
+    if ((rc = dalloc(&c->d_uprev, nb)) || (rc = dalloc(&c->d_fintp, nb)) || (rc = dalloc(&c->d_fextp, nb)) ||
+        (rc = dalloc(&c->d_en, 16 * sizeof(double))) || (rc = dalloc(&c->d_erow, sizeof(int))) ||
+        (rc = dalloc(&c->d_epart, 4 * (size_t)ceil_div(c->npoin, 256) * sizeof(double))))
+      return rc;
+  }
+  if (c->d_ehist) { cudaFree(c->d_ehist); c->d_ehist = nullptr; }
+  if (max_steps > 0 && (rc = dalloc(&c->d_ehist, 5 * (size_t)max_steps * sizeof(double)))) return rc;
+  c->ehist_max = max_steps;
+  // the first balance step measures from the current displacement, with
+  // zero previous forces (fintt/fextt(TIME_N) start at zero)
+  CU(cudaMemcpyAsync(c->d_uprev, c->d_u, nb, cudaMemcpyDeviceToDevice, c->stream));
+  CU(cudaMemsetAsync(c->d_fintp, 0, nb, c->stream));
+  CU(cudaMemsetAsync(c->d_fextp, 0, nb, c->stream));
+  CU(cudaMemsetAsync(c->d_en, 0, 16 * sizeof(double), c->stream));
+  CU(cudaMemsetAsync(c->d_erow, 0, sizeof(int), c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  c->energy = true;
+  return SMA_OK;
+}
+
+int32_t sma_get_energy(sma_ctx* c, double* totals, double* hist, int32_t* nrows) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (!c->d_en) return fail(SMA_ERR_STATE, "energy balance not enabled");
+  CU(cudaSetDevice(c->dev));
+  double h[9];
+  int rows = 0;
+  CU(cudaMemcpyAsync(h, c->d_en, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaMemcpyAsync(&rows, c->d_erow, sizeof rows, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  if (totals) {
+    totals[0] = h[4];
+    totals[1] = h[5];
+    totals[2] = h[6];
+    totals[3] = h[4] + h[6] - h[5];
+    totals[4] = h[7];
+  }
+  rows = std::min(rows, c->ehist_max);
+  if (hist && rows > 0 && c->d_ehist)
+    CU(cudaMemcpy(hist, c->d_ehist, 5 * (size_t)rows * sizeof(double), cudaMemcpyDeviceToHost));
+  if (nrows) *nrows = rows;
+  return SMA_OK;
+}
+
+namespace {
+struct CkptHeader {
+  char magic[8];
+  int32_t version, precision, scheme, has_energy;
+  int64_t nelem, npoin;
+  double cutim;
+};
+}  // namespace
+
+int32_t sma_checkpoint_save(sma_ctx* c, const char* path) {
+  if (!c || !path) return fail(SMA_ERR_ARG, "NULL argument");
+  const size_t n3 = 3 * (size_t)c->npoin;
+  std::vector<double> buf(std::max(n3, 48 * (size_t)c->nelem));
+  CkptHeader hd;
+  std::memset(&hd, 0, sizeof hd);
+  std::memcpy(hd.magic, "SMAB200", 8);
+  hd.version = 1;
+  hd.precision = c->prec;
+  hd.scheme = c->scheme;
+  hd.has_energy = c->energy ? 1 : 0;
+  hd.nelem = c->nelem;
+  hd.npoin = c->npoin;
+  int32_t rc = sma_get_time(c, &hd.cutim);
+  if (rc) return rc;
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(SMA_ERR_ARG, std::string("cannot write ") + path);
+  bool ok = std::fwrite(&hd, sizeof hd, 1, fp) == 1;
+  const int fields[3] = {SMA_FIELD_DISPL, SMA_FIELD_VELOC, SMA_FIELD_ACCEL};
+  for (int q = 0; q < 3 && ok; ++q) {
+    if ((rc = sma_get_nodal(c, fields[q], buf.data()))) { std::fclose(fp); return rc; }
+    ok = std::fwrite(buf.data(), sizeof(double), n3, fp) == n3;
+  }
+  if (ok) {
+    if ((rc = sma_get_state(c, buf.data()))) { std::fclose(fp); return rc; }
+    ok = std::fwrite(buf.data(), sizeof(double), 48 * (size_t)c->nelem, fp) == 48 * (size_t)c->nelem;
+  }
+  if (ok && c->energy) {
+    double* arrs[3] = {c->d_uprev, c->d_fintp, c->d_fextp};
+    for (int q = 0; q < 3 && ok; ++q) {
+      k_soa_to_aos<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(arrs[q], c->d_stage, c->npoin, c->npad);
+      c->launches++;
+      if (cudaMemcpyAsync(buf.data(), c->d_stage, n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+          cudaStreamSynchronize(c->stream) != cudaSuccess) { std::fclose(fp); return fail(SMA_ERR_CUDA, "checkpoint copy"); }
+      ok = std::fwrite(buf.data(), sizeof(double), n3, fp) == n3;
+    }
+    double en[16];
+    if (ok && (cudaMemcpy(en, c->d_en, sizeof en, cudaMemcpyDeviceToHost) != cudaSuccess)) { std::fclose(fp); return fail(SMA_ERR_CUDA, "checkpoint copy"); }
+    if (ok) ok = std::fwrite(en, sizeof(double), 16, fp) == 16;
+  }
+  if (std::fclose(fp) != 0) ok = false;
+  if (!ok) return fail(SMA_ERR_ARG, std::string("short write to ") + path);
+  return SMA_OK;
+}
+
+int32_t sma_checkpoint_load(sma_ctx* c, const char* path) {
+  if (!c || !path) return fail(SMA_ERR_ARG, "NULL argument");
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return fail(SMA_ERR_ARG, std::string("cannot read ") + path);
+  CkptHeader hd;
+  if (std::fread(&hd, sizeof hd, 1, fp) != 1 || std::memcmp(hd.magic, "SMAB200", 8) != 0 || hd.version != 1) {
+    std::fclose(fp);
+    return fail(SMA_ERR_ARG, "not an alya_sma_b200 checkpoint");
+  }
+  if (hd.nelem != c->nelem || hd.npoin != c->npoin || hd.precision != c->prec || hd.scheme != c->scheme) {
+    std::fclose(fp);
+    return fail(SMA_ERR_ARG, "checkpoint of another mesh, precision or scheme");
+  }
+  const size_t n3 = 3 * (size_t)c->npoin;
+  std::vector<double> buf(std::max(n3, 48 * (size_t)c->nelem));
+  const int fields[3] = {SMA_FIELD_DISPL, SMA_FIELD_VELOC, SMA_FIELD_ACCEL};
+  int32_t rc;
+  for (int q = 0; q < 3; ++q) {
+    if (std::fread(buf.data(), sizeof(double), n3, fp) != n3) { std::fclose(fp); return fail(SMA_ERR_ARG, "truncated checkpoint"); }
+    if ((rc = sma_set_nodal(c, fields[q], buf.data()))) { std::fclose(fp); return rc; }
+  }
+  if (std::fread(buf.data(), sizeof(double), 48 * (size_t)c->nelem, fp) != 48 * (size_t)c->nelem) {
+    std::fclose(fp);
+    return fail(SMA_ERR_ARG, "truncated checkpoint");
+  }
+  if ((rc = sma_set_state(c, buf.data()))) { std::fclose(fp); return rc; }
+  if (hd.has_energy) {
+    if ((rc = sma_set_energy(c, 1, c->ehist_max))) { std::fclose(fp); return rc; }
+    double* arrs[3] = {c->d_uprev, c->d_fintp, c->d_fextp};
+    for (int q = 0; q < 3; ++q) {
+      if (std::fread(buf.data(), sizeof(double), n3, fp) != n3) { std::fclose(fp); return fail(SMA_ERR_ARG, "truncated checkpoint"); }
+      CU(cudaMemcpyAsync(c->d_stage, buf.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      k_aos_to_soa<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(c->d_stage, arrs[q], c->npoin, c->npad);
+      c->launches++;
+      CU(cudaStreamSynchronize(c->stream));
+    }
+    double en[16];
+    if (std::fread(en, sizeof(double), 16, fp) != 16) { std::fclose(fp); return fail(SMA_ERR_ARG, "truncated checkpoint"); }
+    CU(cudaMemcpy(c->d_en, en, sizeof en, cudaMemcpyHostToDevice));
+  }
+  std::fclose(fp);
+  return sma_set_time(c, hd.cutim);
 }
 
 int32_t sma_critical_dt(sma_ctx* c, double* dtcri) {
@@ -992,7 +1229,7 @@ __global__ void k_check_lnods(const int32_t* lnods, int64_t n, int32_t npoin, in
 
 template <typename T>
 int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int32_t* d_lnods,
-                    double* d_sdv, cudaStream_t s) {
+                    double* d_sdv, const MatC& mat, cudaStream_t s) {
   const int64_t sst = ceil_div(8 * (int64_t)nelem, 32) * 32;
   T* s_iterk = (T*)(base + NA_OFF_S0);
   T* s_timen = (T*)(base + NA_OFF_S1);
@@ -1006,6 +1243,7 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   a.f = (double*)(base + NA_OFF_F);
   a.lmate = nullptr;
   a.mats = (const MatC*)(base + NA_OFF_MAT);
+  a.mat0 = mat;
   a.tempe = nullptr;
   a.sold = s_timen;
   a.snew = s_iterk;
@@ -1018,7 +1256,7 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   a.end = nelem;
   a.has_grav = 0;
   const int block = 256, epb = block / 8;
-  const size_t smem = (size_t)epb * 9 * sizeof(ElemSmem<T>);
+  const size_t smem = element_smem_bytes<T>(block);
   k_element<T, true><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
   k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
   CU(cudaGetLastError());
@@ -1069,11 +1307,12 @@ extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int3
   const unsigned ngrid = (unsigned)ceil_div(npoin, 256);
   k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_coord, (double*)(base + NA_OFF_COORD), npoin, NA_NPAD);
   k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_displ, (double*)(base + NA_OFF_U), npoin, NA_NPAD);
-  k_put_mat<<<1, 1, 0, s>>>(make_mat(props, e_mart, 1.0), (MatC*)(base + NA_OFF_MAT));
+  const MatC mat = make_mat(props, e_mart, 1.0);
+  k_put_mat<<<1, 1, 0, s>>>(mat, (MatC*)(base + NA_OFF_MAT));
   CU(cudaGetLastError());
   int32_t rc = (precision == SMA_PREC_FP32)
-                   ? noalloc_run<float>(base, nelem, npoin, d_lnods, d_sdv, s)
-                   : noalloc_run<double>(base, nelem, npoin, d_lnods, d_sdv, s);
+                   ? noalloc_run<float>(base, nelem, npoin, d_lnods, d_sdv, mat, s)
+                   : noalloc_run<double>(base, nelem, npoin, d_lnods, d_sdv, mat, s);
   if (rc) return rc;
   k_soa_to_aos<<<ngrid, 256, 0, s>>>((const double*)(base + NA_OFF_F), d_rhsid, npoin, NA_NPAD);
   CU(cudaGetLastError());

@@ -44,6 +44,8 @@ struct StepTime {
   double nx_c_pred;   // t_mid - t of step k+1    (predictor)
   double nx_load;     // load factor at t_{k+1}
   double nx_fval[MAXFUN][3];
+  double load;        // load factor at t_k
+  double phi;         // Tchamwa-Wielgosz parameter (tifac_sld(4))
   int load_fun;
   int pad;
 };
@@ -58,7 +60,7 @@ __device__ __forceinline__ double funbou(const FunTab* ft, int f, int idime, dou
       const double p1 = ft->tab[f][k][1 + idime], p2 = ft->tab[f][k + 1][1 + idime];
       if (ft->smooth[f]) {
         const double m = (cutim - t1) / (t2 - t1);
-        xretu = p1 + (p2 - p1) * pow(m, 3.0) * (10.0 - 15.0 * m + 6.0 * pow(m, 2.0));
+        xretu = p1 + (p2 - p1) * (m * m * m) * (10.0 - 15.0 * m + 6.0 * (m * m));
       } else {
         const double m = (p2 - p1) / (t2 - t1);
         xretu = p1 + m * (cutim - t1);
@@ -72,7 +74,7 @@ __device__ __forceinline__ double funbou(const FunTab* ft, int f, int idime, dou
 }
 
 // corrector constant of step k and predictor data of step k+1
-__device__ __forceinline__ void advance_time(StepTime* ts, const FunTab* ft) {
+__device__ __noinline__ void advance_time(StepTime* ts, const FunTab* ft) {
   const double cutim = ts->cutim, dt = ts->dtime;
   const double t_end = cutim + dt;
   const double t_mid = 0.5 * (cutim + t_end);
@@ -112,36 +114,39 @@ struct ElemArgs {
   int32_t beg, end;            // element range of this launch
   double grav[3];              // rho-scaled body force per unit mass (elfext)
   int has_grav;
+  MatC mat0;                   // the material when lmate is null (kernel-parameter space)
 };
 
+// Shared memory of one element (8 lanes): node data as structure of arrays
+// (phase 1 reads all 8 nodes of one component with 128-bit loads), and the
+// 8 Gauss points' force operators Q (phase 2).  The strides carry a 16-byte
+// pad so the 4 elements of a warp start in different banks.
 template <typename T>
-struct ElemSmem { T v[6]; };
+struct ElemSmem {
+  static constexpr int NODE_STRIDE = 6 * 8 + 16 / sizeof(T);    // elements of T
+  static constexpr int Q_STRIDE = 8 * 12 + 16 / sizeof(T);
+  static constexpr int PER_ELEM = NODE_STRIDE + Q_STRIDE;
+};
 
-// 8-lane butterfly reduce-scatter: f[24] (node-major, 3 comps) summed over
-// the 8 lanes of the element; lane a keeps node a.
+// reference-element table shared by the block: dN_a/dxi_j and N_a at Gauss
+// point g, stored [g][a][4] = (dN/ds, dN/dt, dN/dz, N)
+// Node a of the brick sits at s = +1 for a in {1,2,5,6}, t = +1 for
+// a in {2,3,6,7}, z = +1 for a >= 4 (mod_lagrange.f90:935-977), so its
+// factors and derivative signs follow from the bits of a.
 template <typename T>
-__device__ __forceinline__ void reduce_scatter8(const T* f, int lane8, T* out) {
-  const unsigned FULL = 0xffffffffu;
-  const bool b2 = lane8 & 4, b1 = lane8 & 2, b0 = lane8 & 1;
-  T r12[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) {
-    const T send = b2 ? f[k] : f[12 + k];
-    const T keep = b2 ? f[12 + k] : f[k];
-    r12[k] = keep + __shfl_xor_sync(FULL, send, 4);
-  }
-  T r6[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const T send = b1 ? r12[k] : r12[6 + k];
-    const T keep = b1 ? r12[6 + k] : r12[k];
-    r6[k] = keep + __shfl_xor_sync(FULL, send, 2);
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const T send = b0 ? r6[k] : r6[3 + k];
-    const T keep = b0 ? r6[3 + k] : r6[k];
-    out[k] = keep + __shfl_xor_sync(FULL, send, 1);
+__device__ __forceinline__ void fill_hex8_table(T* tab) {
+  const T p = T(0.577350269189626);
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+    const int g = k >> 3, a = k & 7;
+    const T s = (g & 4) ? p : -p, t = (g & 2) ? p : -p, z = (g & 1) ? p : -p;
+    const int sa = (a ^ (a >> 1)) & 1, ta = (a >> 1) & 1, za = (a >> 2) & 1;
+    const T S = T(0.5) * (sa ? T(1) + s : T(1) - s);
+    const T Tt = T(0.5) * (ta ? T(1) + t : T(1) - t);
+    const T Z = T(0.5) * (za ? T(1) + z : T(1) - z);
+    tab[4 * k + 0] = (sa ? T(0.5) : T(-0.5)) * Tt * Z;
+    tab[4 * k + 1] = (ta ? T(0.5) : T(-0.5)) * S * Z;
+    tab[4 * k + 2] = (za ? T(0.5) : T(-0.5)) * S * Tt;
+    tab[4 * k + 3] = S * Tt * Z;
   }
 }
 
@@ -150,60 +155,77 @@ __device__ __forceinline__ void count_warp(unsigned long long* cnt, int idx, boo
   if (b && (threadIdx.x & 31) == 0) atomicAdd(cnt + idx, (unsigned long long)__popc(b));
 }
 
+// vector loads of 4 consecutive T from shared memory (16-byte aligned)
+__device__ __forceinline__ void lds4(const float* p, float* v) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void lds4(const double* p, double* v) {
+  const double2 a = *reinterpret_cast<const double2*>(p);
+  const double2 b = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// vector loads of 8 consecutive T from shared memory
+__device__ __forceinline__ void lds8(const float* p, float* v) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  const float4 b = *reinterpret_cast<const float4*>(p + 4);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void lds8(const double* p, double* v) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double2 a = *reinterpret_cast<const double2*>(p + 2 * k);
+    v[2 * k] = a.x;
+    v[2 * k + 1] = a.y;
+  }
+}
+
+// Work of one lane (element le, lane a) on one tile once its node is
+// gathered: dX, dU are node a's coordinates and displacement relative to the
+// element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
+// Gauss point a.  Stages the node rows, then phase 1 (lane = Gauss point),
+// the law, phase 2 (lane = node) and the scatter-add.  Needs the block's
+// reference table in `tab`.
 template <typename T, bool ATOMIC>
-__global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
-  extern __shared__ unsigned char smem_raw[];
-  ElemSmem<T>* sm = reinterpret_cast<ElemSmem<T>*>(smem_raw);
-  const int lane8 = threadIdx.x & 7;
-  const int le = threadIdx.x >> 3;
-  const int epb = blockDim.x >> 3;
-  const int64_t e = (int64_t)a.beg + (int64_t)blockIdx.x * epb + le;
-  const bool valid = e < a.end;
-  const int64_t ec = valid ? e : (int64_t)a.end - 1;
-
-  if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
-
-  // gather: lane a loads node a of its element
-  const int nid = a.lnods[8 * ec + lane8];
-  double X[3], U[3];
+__device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab, T* nsm, T* qsm,
+                                             int lane8, bool valid, int64_t ec, int nid,
+                                             const double* dX, const double* dU,
+                                             double xS, double F_AS, double F_SA) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    X[c] = __ldg(a.coord + c * a.npad + nid);
-    U[c] = __ldg(a.u + c * a.npad + nid);
+    nsm[8 * c + lane8] = (T)dX[c];
+    nsm[8 * (3 + c) + lane8] = (T)dU[c];
   }
-  // 9 slots per element (one pad slot) keep the 4 elements of a warp in
-  // different shared-memory banks
-  const int src = (threadIdx.x & 31) & ~7;
-  ElemSmem<T>& mine = sm[le * 9 + lane8];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double x0 = __shfl_sync(0xffffffffu, X[c], src);
-    const double u0 = __shfl_sync(0xffffffffu, U[c], src);
-    mine.v[c] = (T)(X[c] - x0);
-    mine.v[3 + c] = (T)(U[c] - u0);
-  }
-  __syncwarp();
-  const ElemSmem<T>* en = sm + le * 9;
+  const int64_t gp = 8 * ec + lane8;
+  const int im = a.lmate ? a.lmate[ec] : 0;
+  const double tmp = a.tempe ? a.tempe[ec] : 0.0;
+  __syncwarp();                                                  // node rows of the element
 
-  // geometry and displacement gradient at Gauss point g = lane8
-  T N[8], dN[24];
-  hex8_gp<T>(lane8, N, dN);
+  // ---- phase 1, lane = Gauss point g: J = dX/dxi, Gu = du/dxi ------------
   T J[9], Gu[9];
+  {
+    // this lane's Gauss point: derivatives in registers (a table row per
+    // lane would put the 8 lanes of an element in one shared-memory bank)
+    T N[8], dN[24];
+    hex8_gp<T>(lane8, N, dN);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) { J[k] = T(0); Gu[k] = T(0); }
+    for (int k = 0; k < 9; ++k) { J[k] = T(0); Gu[k] = T(0); }
 #pragma unroll
-  for (int n = 1; n < 8; ++n) {
-    const ElemSmem<T> nd = en[n];
+    for (int c = 0; c < 6; ++c) {
+      T v[8];
+      lds8(nsm + 8 * c, v);
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        J[3 * i + j] += nd.v[i] * dN[3 * n + j];
-        Gu[3 * i + j] += nd.v[3 + i] * dN[3 * n + j];
+      for (int n = 1; n < 8; ++n) {
+        T* acc = (c < 3) ? J + 3 * c : Gu + 3 * (c - 3);
+        acc[0] += v[n] * dN[3 * n + 0];
+        acc[1] += v[n] * dN[3 * n + 1];
+        acc[2] += v[n] * dN[3 * n + 2];
       }
+    }
   }
   T Ji[9];
-  const T detJ = inv3(J, Ji);         // Ji[3j+k] = dxi_j/dX_k
+  const T detJ = inv3(J, Ji);                                    // Ji[3j+k] = dxi_j/dX_k
   T H[9];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -211,12 +233,9 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
     for (int k = 0; k < 3; ++k)
       H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
 
-  // constitutive update
-  const int im = a.lmate ? a.lmate[ec] : 0;
-  const MatC& mat = a.mats[im];
-  const double tmp = a.tempe ? a.tempe[ec] : 0.0;
-  const int64_t gp = 8 * ec + lane8;
-  double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp], F_SA = (double)a.sold[2 * a.sst + gp];
+  // ---- constitutive update ----------------------------------------------
+  // one material: constants come from the kernel parameters, no loads
+  const MatC& mat = a.lmate ? a.mats[im] : a.mat0;
   T tau[6];
   const int flag = law160_tau<T>(mat, H, tmp, xS, F_AS, F_SA, tau);
   if (valid) {
@@ -225,49 +244,61 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
     a.snew[2 * a.sst + gp] = (T)F_SA;
   }
 
-  // P = tau F^-T; element force f_a = P gpcar_a vol = vol tau (F J)^-T dN_a
+  // ---- force operator Q = vol tau (F J)^-T, f_a = -Q dN_a ---------------
   T Fm[9], Fi[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) Fm[k] = H[k];
   Fm[0] += T(1); Fm[4] += T(1); Fm[8] += T(1);
   const T detF = inv3(Fm, Fi);
-  T B[9];                              // B = Ji Fi = (F J)^-1
+  T B[9];                                                        // B = Ji Fi = (F J)^-1
 #pragma unroll
   for (int m = 0; m < 3; ++m)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       B[3 * m + k] = Ji[3 * m + 0] * Fi[0 + k] + Ji[3 * m + 1] * Fi[3 + k] + Ji[3 * m + 2] * Fi[6 + k];
-  const T vol = detJ;                  // Gauss weight 1
+  const T vol = detJ;                                            // Gauss weight 1
   const T t00 = tau[0] * vol, t11 = tau[1] * vol, t22 = tau[2] * vol;
   const T t01 = tau[3] * vol, t12 = tau[4] * vol, t02 = tau[5] * vol;
-  T Q[9];                              // Q[3i+m] = vol sum_k tau(i,k) B[3m+k]
+  T* q = qsm + 12 * lane8;
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
-    Q[0 + m] = t00 * B[3 * m + 0] + t01 * B[3 * m + 1] + t02 * B[3 * m + 2];
-    Q[3 + m] = t01 * B[3 * m + 0] + t11 * B[3 * m + 1] + t12 * B[3 * m + 2];
-    Q[6 + m] = t02 * B[3 * m + 0] + t12 * B[3 * m + 1] + t22 * B[3 * m + 2];
+    q[0 + m] = t00 * B[3 * m + 0] + t01 * B[3 * m + 1] + t02 * B[3 * m + 2];
+    q[3 + m] = t01 * B[3 * m + 0] + t11 * B[3 * m + 1] + t12 * B[3 * m + 2];
+    q[6 + m] = t02 * B[3 * m + 0] + t12 * B[3 * m + 1] + t22 * B[3 * m + 2];
   }
-  T fe[24];                            // element residual contribution: -f_int (+ f_ext)
+  q[9] = vol * (T)mat.densi;
+  __syncwarp();
+
+  // ---- phase 2, lane = node a: sum the 8 Gauss points ---------------------
+  T f0 = T(0), f1 = T(0), f2 = T(0);
+  const T gx = (T)a.grav[0], gy = (T)a.grav[1], gz = (T)a.grav[2];
 #pragma unroll
-  for (int n = 0; n < 8; ++n)
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-      fe[3 * n + i] = -(Q[3 * i + 0] * dN[3 * n + 0] + Q[3 * i + 1] * dN[3 * n + 1] + Q[3 * i + 2] * dN[3 * n + 2]);
-  if (a.has_grav) {
-    const T rv = (T)mat.densi * vol;
-#pragma unroll
-    for (int n = 0; n < 8; ++n)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) fe[3 * n + i] += (N[n] * rv) * (T)a.grav[i];
+  for (int g = 0; g < 8; ++g) {
+    T qg[12], dn[4];
+    lds4(qsm + 12 * g, qg);                                      // rows shared by the element
+    lds4(qsm + 12 * g + 4, qg + 4);
+    lds4(qsm + 12 * g + 8, qg + 8);
+    lds4(tab + 32 * g + 4 * lane8, dn);                          // consecutive across lanes
+    f0 -= qg[0] * dn[0] + qg[1] * dn[1] + qg[2] * dn[2];
+    f1 -= qg[3] * dn[0] + qg[4] * dn[1] + qg[5] * dn[2];
+    f2 -= qg[6] * dn[0] + qg[7] * dn[1] + qg[8] * dn[2];
+    if (a.has_grav) {
+      const T w = dn[3] * qg[9];
+      f0 += w * gx;
+      f1 += w * gy;
+      f2 += w * gz;
+    }
   }
-  T out[3];
-  reduce_scatter8<T>(fe, lane8, out);
   if (valid) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double* dst = a.f + c * a.npad + nid;
-      if (ATOMIC) atomicAdd(dst, (double)out[c]);
-      else *dst += (double)out[c];
+    double* dst = a.f + nid;
+    if (ATOMIC) {
+      atomicAdd(dst, (double)f0);
+      atomicAdd(dst + a.npad, (double)f1);
+      atomicAdd(dst + 2 * a.npad, (double)f2);
+    } else {
+      dst[0] += (double)f0;
+      dst[a.npad] += (double)f1;
+      dst[2 * a.npad] += (double)f2;
     }
   }
   count_warp(a.cnt, CNT_NR_ACTIVE, valid && (flag & (NR_CONVERGED | NR_FAILED)));
@@ -276,13 +307,165 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
   count_warp(a.cnt, CNT_NEG_DET, valid && !(detF > T(0)));
 }
 
+// One tile of elements per block: each lane gathers its node with __ldg,
+// takes node 1's values from lane 0 of its element by shuffle.
+template <typename T, bool ATOMIC>
+__global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tab = reinterpret_cast<T*>(smem_raw);                       // [8][8][4]
+  T* elem_sm = tab + 256;
+  const int lane8 = threadIdx.x & 7;
+  const int le = threadIdx.x >> 3;
+  const int epb = blockDim.x >> 3;
+  const int64_t e = (int64_t)a.beg + (int64_t)blockIdx.x * epb + le;
+  const bool valid = e < a.end;
+  const int64_t ec = valid ? e : (int64_t)a.end - 1;
+  T* nsm = elem_sm + le * ElemSmem<T>::PER_ELEM;                 // node rows [6][8]
+  T* qsm = nsm + ElemSmem<T>::NODE_STRIDE;                       // Q rows [8][12]
+
+  if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
+  fill_hex8_table<T>(tab);
+
+  const int nid = a.lnods[8 * ec + lane8];
+  double X[3], U[3], dX[3], dU[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    X[c] = __ldg(a.coord + c * a.npad + nid);
+    U[c] = __ldg(a.u + c * a.npad + nid);
+  }
+  const int src = (threadIdx.x & 31) & ~7;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    dX[c] = X[c] - __shfl_sync(0xffffffffu, X[c], src);
+    dU[c] = U[c] - __shfl_sync(0xffffffffu, U[c], src);
+  }
+  const int64_t gp = 8 * ec + lane8;
+  const double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp];
+  const double F_SA = (double)a.sold[2 * a.sst + gp];
+  __syncthreads();                                               // reference table
+  element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent element kernel: each block walks tiles blockIdx.x, +gridDim.x,
+// ...; while it computes tile t, cp.async copies the node data and state of
+// tile t+1 into a second shared-memory stage and the connectivity of tile t+2
+// is already in a register, so the dependent gather (lnods -> coord, displ)
+// is off the critical path.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// one stage per element: 8 lanes x (X[3], U[3]) doubles, then 8 x 3 state T
+template <typename T>
+struct PipeStage {
+  static constexpr int NODE_DOUBLES = 8 * 6;
+  static constexpr int BYTES = NODE_DOUBLES * 8 + 8 * 4 * sizeof(T);   // state padded to 4
+};
+
+template <typename T, bool ATOMIC>
+__global__ void __launch_bounds__(256) k_element_pipe(ElemArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tab = reinterpret_cast<T*>(smem_raw);
+  T* elem_sm = tab + 256;
+  const int lane8 = threadIdx.x & 7;
+  const int le = threadIdx.x >> 3;
+  const int epb = blockDim.x >> 3;
+  T* nsm = elem_sm + le * ElemSmem<T>::PER_ELEM;
+  T* qsm = nsm + ElemSmem<T>::NODE_STRIDE;
+  unsigned char* stages = reinterpret_cast<unsigned char*>(elem_sm + epb * ElemSmem<T>::PER_ELEM);
+  const int64_t n = (int64_t)a.end - a.beg;
+  const int64_t ntiles = (n + epb - 1) / epb;
+
+  if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
+  fill_hex8_table<T>(tab);
+  __syncthreads();
+  int64_t t = blockIdx.x;
+  if (t >= ntiles) return;                                       // uniform across the block
+
+  auto elem = [&](int64_t tile, bool& v) -> int64_t {
+    const int64_t e = (int64_t)a.beg + tile * epb + le;
+    v = e < a.end;
+    return v ? e : (int64_t)a.end - 1;
+  };
+  auto stage_ptr = [&](int s) -> unsigned char* {
+    return stages + ((size_t)s * epb + le) * PipeStage<T>::BYTES;
+  };
+  auto issue = [&](int s, int nid, int64_t ec) {
+    unsigned char* st = stage_ptr(s);
+    double* nd = reinterpret_cast<double*>(st) + 6 * lane8;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cp_async(nd + c, a.coord + c * a.npad + nid, 8);
+      cp_async(nd + 3 + c, a.u + c * a.npad + nid, 8);
+    }
+    T* ss = reinterpret_cast<T*>(st + PipeStage<T>::NODE_DOUBLES * 8) + 4 * lane8;
+    const int64_t gp = 8 * ec + lane8;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cp_async(ss + c, a.sold + c * a.sst + gp, (int)sizeof(T));
+  };
+
+  bool v0, v1;
+  int64_t ec0 = elem(t, v0);
+  int nid0 = a.lnods[8 * ec0 + lane8];
+  issue(0, nid0, ec0);
+  cp_async_commit();
+  int64_t t1 = t + gridDim.x;
+  int64_t ec1 = elem(t1 < ntiles ? t1 : t, v1);
+  int nid1 = a.lnods[8 * ec1 + lane8];
+  int s = 0;
+  for (; t < ntiles; t += gridDim.x) {
+    const int64_t tn = t + gridDim.x;
+    if (tn < ntiles) issue(s ^ 1, nid1, ec1);
+    cp_async_commit();
+    const int64_t tn2 = tn + gridDim.x;
+    bool v2;
+    const int64_t ec2 = elem(tn2 < ntiles ? tn2 : t, v2);
+    const int nid2 = a.lnods[8 * ec2 + lane8];
+    cp_async_wait1();                                            // this tile's copies landed
+    __syncwarp();
+    const unsigned char* st = stage_ptr(s);
+    const double* nd = reinterpret_cast<const double*>(st);
+    const T* ss = reinterpret_cast<const T*>(st + PipeStage<T>::NODE_DOUBLES * 8) + 4 * lane8;
+    double dX[3], dU[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      dX[c] = nd[6 * lane8 + c] - nd[c];                         // relative to node 1 (lane 0)
+      dU[c] = nd[6 * lane8 + 3 + c] - nd[3 + c];
+    }
+    element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, v0, ec0, nid0, dX, dU, (double)ss[0],
+                            (double)ss[1], (double)ss[2]);
+    __syncwarp();                                                // stage s is reused next-but-one
+    nid0 = nid1; ec0 = ec1; v0 = v1;
+    nid1 = nid2; ec1 = ec2; v1 = v2;
+    s ^= 1;
+  }
+  cp_async_wait0();
+}
+
+// dynamic shared memory of the element kernels for a block of `block` threads
+template <typename T>
+inline size_t element_smem_bytes(int block) {
+  return (256 + (size_t)(block / 8) * ElemSmem<T>::PER_ELEM) * sizeof(T);
+}
+template <typename T>
+inline size_t element_pipe_smem_bytes(int block) {
+  return element_smem_bytes<T>(block) + 2 * (size_t)(block / 8) * PipeStage<T>::BYTES;
+}
+
 // ---------------------------------------------------------------------------
 // nodal kernels (FP64): MODE 0 predictor, 1 corrector + next predictor,
 // 2 corrector
 // ---------------------------------------------------------------------------
 struct NodalArgs {
   double* u;          // displacement
-  double* vt;         // velocity at the half step (veloctmp_sld)
+  double* vt;         // CD: velocity at the half step (veloctmp_sld); TW: predicted velocity
   double* v;          // velocity at the step boundary
   double* acc;        // acceleration at the step boundary
   double* f;          // residual accumulator
@@ -292,14 +475,28 @@ struct NodalArgs {
   const double* fext;     // SoA [3][npad] nodal load at factor 1
   StepTime* ts;
   unsigned long long* cnt;
+  // energy balance (ENERGY only): previous displacement and forces, and the
+  // step's partial sums (ALLIE, ALLWK increments, 2*ALLKE, EENER)
+  double* uprev;
+  double* fint_prev;
+  double* fext_prev;
+  double* en_step;
   int64_t npoin, npad;
 };
 
-template <int MODE>
+constexpr int SCHEME_CD = 0, SCHEME_TW = 1;
+
+// MODE 0: predictor of step k+1 from the step-boundary state
+// MODE 1: corrector of step k fused with the predictor of step k+1
+// MODE 2: corrector of step k (leaves the step-boundary state)
+// CD: mod_sld_solution_methods.f90:122-145 (predictor), 192-210 (corrector)
+// TW: mod_sld_solution_methods.f90:406-429 (predictor), 504-527 (corrector)
+template <int MODE, int SCHEME, bool ENERGY>
 __global__ void __launch_bounds__(256) k_nodal(NodalArgs a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p < a.npoin;
   bool bad = false;
+  double e_ie = 0.0, e_wk = 0.0, e_ke = 0.0, e_ee = 0.0;
   if (valid) {
     const StepTime& ts = *a.ts;
     const uint8_t fl = a.flags[p];
@@ -309,42 +506,135 @@ __global__ void __launch_bounds__(256) k_nodal(NodalArgs a) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t k = c * a.npad + p;
+      const bool fixed = fl & (1u << c);
       double vv, aa;
       if (MODE == 0) {
         vv = a.v[k];
         aa = a.acc[k];
       } else {
-        aa = 0.0 + a.f[k] * invm;           // lumped-mass solve
-        vv = a.vt[k] + ts.c_corr * aa;      // corrector
+        const double r = a.f[k];
+        aa = 0.0 + r * invm;                              // lumped-mass solve
         bad |= !isfinite(aa);
+        if (SCHEME == SCHEME_CD) {
+          vv = a.vt[k] + ts.c_corr * aa;                  // CD corrector
+        } else {
+          vv = fixed ? 0.0 : a.vt[k];                     // TW: fixed dofs at rest
+          if (fixed) aa = 0.0;
+        }
+        if (ENERGY) {                                     // mod_sld_energy.f90:71-193
+          const double uk = a.u[k];
+          const double fx = (fl & 8u) ? a.fext[k] * ts.load : 0.0;
+          const double fi = fx - r;
+          const double dd = uk - a.uprev[k];
+          e_ie += (fi + a.fint_prev[k]) * dd;
+          e_wk += (fx + a.fext_prev[k]) * dd;
+          e_ke += vv * vv / invm;
+          e_ee += r * dd;
+          a.uprev[k] = uk;
+          a.fint_prev[k] = fi;
+          a.fext_prev[k] = fx;
+        }
       }
       if (MODE == 2) {
         a.acc[k] = aa;
         a.v[k] = vv;
       } else {
-        const double vt = vv + ts.nx_c_pred * aa;   // predictor of step k+1
-        double un = a.u[k] + dt * vt;
-        if (fl & (1u << c)) {
+        double vn, un;
+        if (SCHEME == SCHEME_CD) {
+          vn = vv + ts.nx_c_pred * aa;                    // v at the half step k+1/2
+          un = a.u[k] + dt * vn;
+        } else {
+          vn = vv + dt * aa;                              // TW predictor
+          un = a.u[k] + dt * vv + ts.phi * (dt * dt) * aa;
+        }
+        if (fixed) {
           const int fn = a.bcfun[p];
           un = (fn >= 0) ? ts.nx_fval[fn][c] : 0.0;
         }
-        a.vt[k] = vt;
+        a.vt[k] = vn;
         a.u[k] = un;
         a.f[k] = (fl & 8u) ? a.fext[k] * ts.nx_load : 0.0;
       }
     }
   }
   if (MODE >= 1) count_warp(a.cnt, CNT_NONFINITE, valid && bad);
-  if (MODE != 2 && blockIdx.x == 0 && threadIdx.x == 0) a.ts->cutim = a.ts->nx_cutim;
+  if (ENERGY && MODE >= 1) {
+    // fixed-order sums (warp butterfly, then the block's 8 warps in order)
+    // into one partial per block, so the balance is bitwise reproducible
+    __shared__ double wsum[8][4];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      e_ie += __shfl_xor_sync(0xffffffffu, e_ie, o);
+      e_wk += __shfl_xor_sync(0xffffffffu, e_wk, o);
+      e_ke += __shfl_xor_sync(0xffffffffu, e_ke, o);
+      e_ee += __shfl_xor_sync(0xffffffffu, e_ee, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      const int w = threadIdx.x >> 5;
+      wsum[w][0] = e_ie; wsum[w][1] = e_wk; wsum[w][2] = e_ke; wsum[w][3] = e_ee;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += wsum[w][threadIdx.x];
+      a.en_step[4 * (int64_t)blockIdx.x + threadIdx.x] = s;
+    }
+  }
+  if (MODE != 2 && blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ts->cutim = a.ts->nx_cutim;
+    a.ts->load = a.ts->nx_load;
+  }
 }
 
-// witness: displacement of selected dofs after a step
-__global__ void k_witness(const double* u, int64_t npad, const int32_t* wdof, int nwit,
-                          double* hist, int* row, int max_rows) {
+// energy totals after a step (mod_sld_energy.f90:130-157): increments are
+// taken in absolute value, halved except on the first step; one history row
+// (ALLIE, ALLWK, ALLKE, ETOTA, EENER) per step
+// one block of 256 threads: the nodal kernel's per-block partials summed in
+// a fixed order (strided per thread, then a tree), then the totals
+__global__ void __launch_bounds__(256) k_energy_finalize(const double* part, int nblocks,
+                                                         double* en_tot, double* hist, int* row,
+                                                         int max_rows) {
+  __shared__ double red[256][4];
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += 256)
+    for (int q = 0; q < 4; ++q) s[q] += part[4 * (int64_t)b + q];
+  for (int q = 0; q < 4; ++q) red[threadIdx.x][q] = s[q];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int q = 0; q < 4; ++q) red[threadIdx.x][q] += red[threadIdx.x + w][q];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const bool first = en_tot[4] == 0.0;
+  const double w = first ? 1.0 : 0.5;
+  en_tot[0] += w * fabs(red[0][0]);
+  en_tot[1] += w * fabs(red[0][1]);
+  en_tot[2] = 0.5 * red[0][2];
+  en_tot[3] = fabs(red[0][3]);
+  en_tot[4] += 1.0;
+  const int r = *row;
+  if (hist && r < max_rows) {
+    double* h = hist + 5 * (int64_t)r;
+    h[0] = en_tot[0];
+    h[1] = en_tot[1];
+    h[2] = en_tot[2];
+    h[3] = en_tot[0] + en_tot[2] - en_tot[1];
+    h[4] = en_tot[3];
+  }
+  *row = r + 1;
+}
+
+// witness: after the element loop of a step, record displacement (ids in
+// [0, 3 npoin)) or residual (ids in [3 npoin, 6 npoin)) of selected dofs
+__global__ void k_witness(const double* u, const double* f, int64_t npoin, int64_t npad,
+                          const int32_t* wdof, int nwit, double* hist, int* row, int max_rows) {
   const int r = *row;
   for (int w = threadIdx.x; w < nwit; w += blockDim.x) {
-    const int d = wdof[w];
-    if (r < max_rows) hist[(int64_t)r * nwit + w] = u[(int64_t)(d % 3) * npad + d / 3];
+    int d = wdof[w];
+    const double* src = u;
+    if (d >= 3 * npoin) { d -= (int)(3 * npoin); src = f; }
+    if (r < max_rows) hist[(int64_t)r * nwit + w] = src[(int64_t)(d % 3) * npad + d / 3];
   }
   __syncthreads();
   if (threadIdx.x == 0) *row = r + 1;

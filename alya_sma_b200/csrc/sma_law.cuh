@@ -41,43 +41,76 @@ struct MatC {
   double alfa, C_AS, C_SA;      // alpha, Clausius-Clapeyron slopes
   double Rs_AS, Rf_AS, Rs_SA, Rf_SA;
   double EA, EM, nu;            // extension: Reuss modulus E(xS0) when EM != EA
+  double iEA, iEM;              // 1/EA, 1/EM
+  double kK, kG;                // 1/(3 - 6 nu), 1/(2 + 2 nu)
   double densi;
   int ext_E;                    // 1: E depends on xS0
   int pad;
 };
 
 // ---------------------------------------------------------------------------
-// scalar helpers
+// scalar helpers.  Fm<double> calls the accurate library functions; Fm<float>
+// (the precision form) uses fast reciprocals and short series whose error
+// stays at a few FP32 ulp on the ranges they are used on.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float  dlog1p(float x)  { return log1pf(x); }
-__device__ __forceinline__ double dlog1p(double x) { return log1p(x); }
-__device__ __forceinline__ float  dsqrt(float x)   { return sqrtf(x); }
-__device__ __forceinline__ double dsqrt(double x)  { return sqrt(x); }
-__device__ __forceinline__ float  dacos(float x)   { return acosf(x); }
-__device__ __forceinline__ double dacos(double x)  { return acos(x); }
-__device__ __forceinline__ void dsincos(float x, float* s, float* c)    { sincosf(x, s, c); }
-__device__ __forceinline__ void dsincos(double x, double* s, double* c) { sincos(x, s, c); }
+template <typename T> struct Fm;
 
-template <typename T> struct Eps;
-template <> struct Eps<float>  {
-  static __device__ __forceinline__ float series() { return 1e-3f; }   // |w| below: series
-  static __device__ __forceinline__ float dd2()    { return 1e-4f; }   // clustered spread
-};
-template <> struct Eps<double> {
-  static __device__ __forceinline__ double series() { return 1e-3; }
-  static __device__ __forceinline__ double dd2()    { return 1e-8; }
-};
-
-// log1p(w)/w, accurate for all w > -1 (series below |w| < 1e-3: the
-// truncation error w^7/8 < 1.3e-22).
-template <typename T>
-__device__ __forceinline__ T log1p_ratio(T w) {
-  if (fabs(w) < Eps<T>::series()) {
-    return T(1) + w * (T(-0.5) + w * (T(1) / T(3) + w * (T(-0.25) + w * (T(0.2) +
-           w * (T(-1) / T(6) + w * (T(1) / T(7)))))));
+template <> struct Fm<double> {
+  static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+  static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+  static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double acos_(double x) { return acos(x); }
+  static __device__ __forceinline__ double log1p_(double x) { return log1p(x); }
+  // log1p(w)/w; series below |w| < 1e-3 (truncation w^7/8 < 1.3e-22)
+  static __device__ __forceinline__ double log1p_ratio(double w) {
+    if (fabs(w) < 1e-3)
+      return 1.0 + w * (-0.5 + w * (1.0 / 3.0 + w * (-0.25 + w * (0.2 + w * (-1.0 / 6.0 + w * (1.0 / 7.0))))));
+    return log1p(w) / w;
   }
-  return dlog1p(w) / w;
-}
+  // cos and sin of phi in [0, pi/3] by Taylor series (truncation < 1e-18)
+  static __device__ __forceinline__ void sincos_third(double x, double* s, double* c) {
+    const double x2 = x * x;
+    *c = 1.0 + x2 * (-1.0 / 2 + x2 * (1.0 / 24 + x2 * (-1.0 / 720 + x2 * (1.0 / 40320 + x2 * (-1.0 / 3628800 +
+         x2 * (1.0 / 479001600 + x2 * (-1.0 / 87178291200.0 + x2 * (1.0 / 20922789888000.0 +
+         x2 * (-1.0 / 6402373705728000.0)))))))));
+    *s = x * (1.0 + x2 * (-1.0 / 6 + x2 * (1.0 / 120 + x2 * (-1.0 / 5040 + x2 * (1.0 / 362880 +
+         x2 * (-1.0 / 39916800 + x2 * (1.0 / 6227020800.0 + x2 * (-1.0 / 1307674368000.0 +
+         x2 * (1.0 / 355687428096000.0 + x2 * (-1.0 / 121645100408832000.0))))))))));
+  }
+  static __device__ __forceinline__ double clustered() { return 1e-8; }
+};
+
+template <> struct Fm<float> {
+  static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+  static __device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+  static __device__ __forceinline__ float acos_(float x) { return acosf(x); }
+  // log1p(x) = 2 atanh(s), s = x/(2+x): series to s^9 for |x| <= 0.25
+  // (|s| <= 1/7, truncation 2 s^11/11 < 6e-11 relative)
+  static __device__ __forceinline__ float log1p_(float x) {
+    if (fabsf(x) > 0.25f) return log1pf(x);
+    const float s = __fdividef(x, 2.0f + x);
+    const float s2 = s * s;
+    return 2.0f * s * (1.0f + s2 * (1.0f / 3 + s2 * (1.0f / 5 + s2 * (1.0f / 7 + s2 * (1.0f / 9)))));
+  }
+  // log1p(w)/w = 2/(2+w) * (1 + s^2/3 + s^4/5 + ...), stable through w = 0
+  static __device__ __forceinline__ float log1p_ratio(float w) {
+    if (fabsf(w) > 0.25f) return __fdividef(log1pf(w), w);
+    const float r = __fdividef(1.0f, 2.0f + w);
+    const float s = w * r;
+    const float s2 = s * s;
+    return 2.0f * r * (1.0f + s2 * (1.0f / 3 + s2 * (1.0f / 5 + s2 * (1.0f / 7 + s2 * (1.0f / 9)))));
+  }
+  // cos and sin of phi in [0, pi/3] (truncation < 1e-9)
+  static __device__ __forceinline__ void sincos_third(float x, float* s, float* c) {
+    const float x2 = x * x;
+    *c = 1.0f + x2 * (-1.0f / 2 + x2 * (1.0f / 24 + x2 * (-1.0f / 720 + x2 * (1.0f / 40320 +
+         x2 * (-1.0f / 3628800 + x2 * (1.0f / 479001600))))));
+    *s = x * (1.0f + x2 * (-1.0f / 6 + x2 * (1.0f / 120 + x2 * (-1.0f / 5040 + x2 * (1.0f / 362880 +
+         x2 * (-1.0f / 39916800))))));
+  }
+  static __device__ __forceinline__ float clustered() { return 1e-4f; }
+};
 
 // ---------------------------------------------------------------------------
 // log1p of a symmetric 3x3 matrix.  A, L stored as (xx, yy, zz, xy, yz, xz).
@@ -85,20 +118,21 @@ __device__ __forceinline__ T log1p_ratio(T w) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void sym_log1p(const T* A, T* L, T* f) {
+  using M = Fm<T>;
   const T m = (A[0] + A[1] + A[2]) * (T(1) / T(3));
   const T a0 = A[0] - m, a1 = A[1] - m, a2 = A[2] - m;
   const T off = A[3] * A[3] + A[4] * A[4] + A[5] * A[5];
   const T p2 = (a0 * a0 + a1 * a1 + a2 * a2 + T(2) * off) * (T(1) / T(6));
-  const T p = dsqrt(p2);
+  const T p = M::sqrt_(p2);
   // det(A - m I)
   const T det = a0 * (a1 * a2 - A[4] * A[4]) - A[3] * (A[3] * a2 - A[4] * A[5])
               + A[5] * (A[3] * A[4] - a1 * A[5]);
-  T r = (p2 > T(1e-30)) ? det / (T(2) * p2 * p) : T(0);
+  T r = (p2 > T(1e-30)) ? M::div(det, T(2) * p2 * p) : T(0);
   r = fmin(fmax(r, T(-1)), T(1));
-  const T phi = dacos(r) * (T(1) / T(3));
+  const T phi = M::acos_(r) * (T(1) / T(3));
   T sn, cs;
-  dsincos(phi, &sn, &cs);
-  const T d0 = m + T(2) * p * cs;                                          // largest
+  M::sincos_third(phi, &sn, &cs);
+  const T d0 = m + T(2) * p * cs;                                               // largest
   const T d2 = m + T(2) * p * (T(-0.5) * cs - T(0.86602540378443864676) * sn);  // smallest
   const T d1 = T(3) * m - d0 - d2;
   // (u, v): the closest pair, s: the remaining eigenvalue
@@ -106,17 +140,16 @@ __device__ __forceinline__ void sym_log1p(const T* A, T* L, T* f) {
   const T u = lo ? d0 : d1;
   const T v = lo ? d1 : d2;
   const T s = lo ? d2 : d0;
-  const T fu = dlog1p(u), fv = dlog1p(v), fs = dlog1p(s);
+  const T fu = M::log1p_(u), fv = M::log1p_(v), fs = M::log1p_(s);
   f[0] = fs; f[1] = fu; f[2] = fv;
-  const T iv = T(1) / (T(1) + v);
-  const T fuv = log1p_ratio((u - v) * iv) * iv;              // f[u,v]
-  const T fsv = log1p_ratio((s - v) * iv) * iv;              // f[s,v]
+  const T iv = M::rcp(T(1) + v);
+  const T fuv = M::log1p_ratio((u - v) * iv) * iv;              // f[u,v]
+  const T fsv = M::log1p_ratio((s - v) * iv) * iv;              // f[s,v]
   const T dsu = s - u;
-  T fsuv;                                                    // f[s,u,v]
-  if (fabs(dsu) > Eps<T>::dd2()) fsuv = (fsv - fuv) / dsu;
-  else { const T q = T(1) / (T(1) + m); fsuv = T(-0.5) * q * q; }
-  // L = fv I + f[u,v] (A - v I) + f[s,u,v] (A - u I)(A - v I)
-  //   = c0 I + c1 A + c2 A^2
+  T fsuv;                                                       // f[s,u,v]
+  if (fabs(dsu) > M::clustered()) fsuv = M::div(fsv - fuv, dsu);
+  else { const T q = M::rcp(T(1) + m); fsuv = T(-0.5) * q * q; }
+  // L = fv I + f[u,v] (A - v I) + f[s,u,v] (A - u I)(A - v I) = c0 I + c1 A + c2 A^2
   const T c2 = fsuv;
   const T c1 = fuv - fsuv * (u + v);
   const T c0 = fv - fuv * v + fsuv * u * v;
@@ -167,16 +200,19 @@ __device__ __forceinline__ RMOut return_map(const MatC& m, double K, double G, d
     int iter = 0;
     double RHS_AS = (F_AS - m.Rf_AS) * dh_AS + H_AS * F_AS_dot * (1.0 - xS);
     double RHS_SA = (F_SA - m.Rf_SA) * dh_SA - H_SA * F_SA_dot * xS;
-    double resi = RHS_AS * RHS_AS + RHS_SA * RHS_SA;
-    while (iter < 65 && resi > 1.0e-8) {
+    // the reference tests the squared residual on entry (:403) and the norm
+    // in the loop (:454); norm > 1e-8 is tested as squared norm > 1e-16
+    double r2 = RHS_AS * RHS_AS + RHS_SA * RHS_SA;
+    bool go = r2 > 1.0e-8;
+    while (iter < 65 && go) {
       ++iter;
       const double m11 = -G_1 * dh_AS - (H_AS * F_AS_dot + H_AS * (1.0 - xS) * G_1) + (F_AS - m.Rf_AS);
       const double m12 = -G_1 * dh_AS - (H_AS * F_AS_dot + H_AS * (1.0 - xS) * G_1);
       const double m21 = -G_1 * dh_SA - (H_SA * F_SA_dot - H_SA * xS * G_1);
       const double m22 = -G_1 * dh_SA - (H_SA * F_SA_dot - H_SA * xS * G_1) + (F_SA - m.Rf_SA);
-      const double det = m11 * m22 - m12 * m21;
-      const double sol1 = (m22 / det) * RHS_AS + (-m12 / det) * RHS_SA;
-      const double sol2 = (-m21 / det) * RHS_AS + (m11 / det) * RHS_SA;
+      const double rdet = 1.0 / (m11 * m22 - m12 * m21);
+      const double sol1 = (m22 * RHS_AS - m12 * RHS_SA) * rdet;
+      const double sol2 = (m11 * RHS_SA - m21 * RHS_AS) * rdet;
       dh_AS = dh_AS - sol1;
       dh_SA = dh_SA - sol2;
       xS = xS + dh_SA + dh_AS;
@@ -186,7 +222,8 @@ __device__ __forceinline__ RMOut return_map(const MatC& m, double K, double G, d
       F_SA_dot = F_SA - F_SA_0;
       RHS_AS = (F_AS - m.Rf_AS) * dh_AS + H_AS * F_AS_dot * (1.0 - xS);
       RHS_SA = (F_SA - m.Rf_SA) * dh_SA - H_SA * F_SA_dot * xS;
-      resi = sqrt(RHS_AS * RHS_AS + RHS_SA * RHS_SA);
+      r2 = RHS_AS * RHS_AS + RHS_SA * RHS_SA;
+      go = r2 > 1.0e-16;
     }
     if (iter >= 65) {
       o.flag |= NR_FAILED;
@@ -206,12 +243,14 @@ __device__ __forceinline__ RMOut return_map(const MatC& m, double K, double G, d
 }
 
 // ---------------------------------------------------------------------------
-// Kirchhoff stress of law 160 from H = F - I.  state = (xS, F_AS, F_SA) of
-// the previous step; on return the new state.  tau as (xx,yy,zz,xy,yz,xz).
+// Kirchhoff stress of law 160 from H = F - I (row-major).  state = (xS, F_AS,
+// F_SA) of the previous step; on return the new state.  tau as
+// (xx, yy, zz, xy, yz, xz).
 // ---------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
                                           double& xS, double& F_AS, double& F_SA, T* tau) {
+  using M = Fm<T>;
   // A = b - I = H + H^T + H H^T, H row-major (H[3i+j] = du_i/dX_j)
   T A[6];
   A[0] = T(2) * H[0] + (H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
@@ -226,13 +265,13 @@ __device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
   const T theta_t = T(0.5) * (f[0] + f[1] + f[2]);
   const T t3 = theta_t * (T(1) / T(3));
   const T e0 = T(0.5) * f[0] - t3, e1 = T(0.5) * f[1] - t3, e2 = T(0.5) * f[2] - t3;
-  const T en_t = dsqrt(e0 * e0 + e1 * e1 + e2 * e2);
+  const T en_t = M::sqrt_(e0 * e0 + e1 * e1 + e2 * e2);
   // moduli (extension: Reuss E at the start-of-step fraction)
   double K = m.K, G = m.G, G_1 = m.G1;
   if (m.ext_E) {
-    const double E = 1.0 / ((1.0 - xS) / m.EA + xS / m.EM);
-    K = E / (3.0 - 6.0 * m.nu);
-    G = E / (2.0 + 2.0 * m.nu);
+    const double E = 1.0 / ((1.0 - xS) * m.iEA + xS * m.iEM);
+    K = E * m.kK;
+    G = E * m.kG;
     G_1 = (2.0 * G + 9.0 * (m.alfa * m.alfa) * K) * m.eL;
   }
   const double theta = (double)theta_t, e_n = (double)en_t;
@@ -241,16 +280,17 @@ __device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
   F_AS = r.F_AS;
   F_SA = r.F_SA;
   // tau = pv I + kappa (L/2 - theta/3 I)   (:487-491)
-  const double pv = K * (theta - 3.0 * m.alfa * m.eL * xS);
-  const double kap = (e_n > 2.220446049250313e-16) ? 2.0 * G * (1.0 - m.eL * xS / e_n) : 2.0 * G;
-  const T kp = (T)kap;
-  const T dg = (T)pv - kp * t3;
-  tau[0] = dg + kp * T(0.5) * L[0];
-  tau[1] = dg + kp * T(0.5) * L[1];
-  tau[2] = dg + kp * T(0.5) * L[2];
-  tau[3] = kp * T(0.5) * L[3];
-  tau[4] = kp * T(0.5) * L[4];
-  tau[5] = kp * T(0.5) * L[5];
+  const T pv = (T)(K * (theta - 3.0 * m.alfa * m.eL * xS));
+  const T twoG = (T)(2.0 * G);
+  const T kp = (en_t > T(2.220446049250313e-16)) ? twoG * (T(1) - (T)(m.eL * xS) * M::rcp(en_t)) : twoG;
+  const T kh = T(0.5) * kp;
+  const T dg = pv - kp * t3;
+  tau[0] = dg + kh * L[0];
+  tau[1] = dg + kh * L[1];
+  tau[2] = dg + kh * L[2];
+  tau[3] = kh * L[3];
+  tau[4] = kh * L[4];
+  tau[5] = kh * L[5];
   return r.flag;
 }
 
@@ -261,7 +301,7 @@ __device__ __forceinline__ T inv3(const T* M, T* Mi) {
   const T c01 = M[5] * M[6] - M[3] * M[8];
   const T c02 = M[3] * M[7] - M[4] * M[6];
   const T det = M[0] * c00 + M[1] * c01 + M[2] * c02;
-  const T id = T(1) / det;
+  const T id = Fm<T>::rcp(det);
   Mi[0] = c00 * id;
   Mi[3] = c01 * id;
   Mi[6] = c02 * id;

@@ -170,7 +170,8 @@ def ogrid_cylinder(radius, length, n_core, n_ring, n_axial, jitter=0.0, seed=0):
         for r in range(nr):
             k00 = ring_keys[m] if r == 0 else ("r", m, r)
             k10 = ring_keys[m1] if r == 0 else ("r", m1, r)
-            quads.append((k00, k10, ("r", m1, r + 1), ("r", m, r + 1)))
+            # counter-clockwise in (y, z): outward first, then along the ring
+            quads.append((k00, ("r", m, r + 1), ("r", m1, r + 1), k10))
     keys = list(pts.keys())
     index = {kk: n for n, kk in enumerate(keys)}
     xy = np.array([pts[kk] for kk in keys], dtype=np.float64)
@@ -323,6 +324,103 @@ def bar_40x4x4(nsteps=4000, seed=0, ref_equivalent=False, scale=1):
                    fun_smooth=np.array([1], np.int32), fun_tab=tab, dtime=dt, nsteps=nsteps,
                    name="bar_40x4x4" + ("" if scale == 1 else f"_x{scale}"),
                    info=dict(mesh=f"{40*scale}x{4*scale}x{4*scale}", ref_equivalent=ref_equivalent))
+
+
+def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0)):
+    """NiTi cylinder r = 5 mm, L = 50 mm, HEX08 O-grid: a 32x32 core block and
+    four 32x24 ring blocks per cross-section (4,096 cells), 488 layers
+    (1,998,848 elements at div=1; every count divided by div).  Interior nodes
+    jittered U(-0.1,0.1)h.  Every element gets its own material: E_A, E_M,
+    eps_L and the four transformation stresses scaled by U(1-spread, 1+spread)
+    from numpy.random.default_rng(seed).  Temperature rises linearly from
+    t_range[0] at x = 0 to t_range[1] at x = L; the transformation stresses
+    shift by 6.5 MPa/K above 300 K (extension: the reference law has no
+    temperature).  x = 0 clamped; the x = L face is pushed to -3 % axial strain
+    and released with smooth steps over nsteps steps of dt = 0.5 dt_crit."""
+    nc, nr, nx = max(2, 32 // div), max(1, 24 // div), max(2, 488 // div)
+    coord, lnods = ogrid_cylinder(5.0, 50.0, nc, nr, nx, jitter=0.1, seed=seed)
+    ne, npo = lnods.shape[0], coord.shape[0]
+    rng = np.random.default_rng(seed + 1)
+    base = nitinol_props(**NITI, C_AS=6.5 * SQRT_2_3, C_SA=6.5 * SQRT_2_3, T_ref=300.0)
+    props = np.tile(base, (ne, 1))
+    f = rng.uniform(1.0 - spread, 1.0 + spread, size=(ne, 7))
+    props[:, 0] *= f[:, 0]
+    props[:, 2] *= f[:, 1]
+    props[:, 3] *= f[:, 2]
+    props[:, 4] *= f[:, 3]
+    props[:, 9] *= f[:, 4]
+    props[:, 10] *= f[:, 5]
+    e_mart = NITI_E_MART * f[:, 6]
+    densi = np.full(ne, NITI_DENSITY)
+    xc = coord[lnods].mean(axis=1)[:, 0]
+    tempe = t_range[0] + (t_range[1] - t_range[0]) * xc / 50.0
+    fixno = np.zeros((npo, 3), np.int32)
+    bcfun = np.full(npo, -1, np.int32)
+    x0 = face_nodes(coord, 0, 0.0)
+    xl = face_nodes(coord, 0, 50.0)
+    fixno[x0] = 1
+    fixno[xl, 0] = 1
+    bcfun[xl] = 0
+    lmate = np.arange(ne, dtype=np.int32)
+    # E_M (at most 44 GPa here) stays below E_A (at least 54 GPa): E_A sets c
+    dt = 0.5 * critical_dt(coord, lnods, props, densi, lmate)
+    tab = smooth_cycle_table(nsteps * dt, -0.03 * 50.0)
+    return Problem(coord=coord, lnods=lnods, props=props, e_mart=e_mart, densi=densi,
+                   fixno=fixno, bcfun=bcfun, fun_npts=np.array([3], np.int32),
+                   fun_smooth=np.array([1], np.int32), fun_tab=tab, lmate=lmate, tempe=tempe,
+                   dtime=dt, nsteps=nsteps, name=f"cylinder_ogrid_{ne}",
+                   info=dict(mesh=f"O-grid core {nc}x{nc}, ring {nr}, {nx} layers", elements=ne))
+
+
+def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15):
+    """Batched ensemble: nspec independent NiTi specimens (10:1:1 bars, 1 mm
+    elements) with element counts drawn log-uniform in [emin, emax] and every
+    specimen's E_A, E_M, eps_L and transformation stresses scaled by
+    U(1-spread, 1+spread).  Specimens are concatenated into one mesh (disjoint
+    node ranges), so one element launch and one step graph cover all of them.
+    Each is clamped at its x = 0 face and pulled by an axial tip traction of
+    its own amplitude (0.8 to 1.5 times its forward-finish stress) through a
+    shared smooth load cycle; one dt (0.5 dt_crit of the stiffest specimen)."""
+    rng = np.random.default_rng(seed)
+    n_target = np.exp(rng.uniform(np.log(emin), np.log(emax), size=nspec))
+    coords, lnods_l, props_l, em_l, fixno_l, fext_l, spec_of = [], [], [], [], [], [], []
+    off = 0
+    base = nitinol_props(**NITI)
+    for s in range(nspec):
+        k = max(2, int(round((n_target[s] / 10.0) ** (1.0 / 3.0))))
+        nx, ny = 10 * k, k
+        c, l = structured_box(nx, ny, ny, float(nx), float(ny), float(ny), 0.05, seed + 100 + s)
+        f = rng.uniform(1.0 - spread, 1.0 + spread, size=7)
+        pr = base.copy()
+        pr[0] *= f[0]; pr[2] *= f[1]; pr[3] *= f[2]; pr[4] *= f[3]; pr[9] *= f[4]; pr[10] *= f[5]
+        props_l.append(pr)
+        em_l.append(NITI_E_MART * f[6])
+        fx = np.zeros((c.shape[0], 3), np.int32)
+        fx[face_nodes(c, 0, 0.0)] = 1
+        amp = rng.uniform(0.8, 1.5) * pr[4]
+        fe = face_load(c, l, 0, float(nx), (amp, 0.0, 0.0))
+        coords.append(c)
+        lnods_l.append(l + off)
+        fixno_l.append(fx)
+        fext_l.append(fe)
+        spec_of.append(np.full(l.shape[0], s, np.int32))
+        off += c.shape[0]
+    coord = np.concatenate(coords)
+    lnods = np.concatenate(lnods_l).astype(np.int32)
+    lmate = np.concatenate(spec_of)
+    props = np.array(props_l)
+    e_mart = np.array(em_l)
+    densi = np.full(nspec, NITI_DENSITY)
+    fixno = np.concatenate(fixno_l)
+    fext = np.concatenate(fext_l)
+    dt = 0.5 * critical_dt(coord, lnods, props, densi, lmate)
+    tab = smooth_cycle_table(nsteps * dt, 1.0)
+    return Problem(coord=coord, lnods=lnods, props=props, e_mart=e_mart, densi=densi,
+                   fixno=fixno, bcfun=np.full(coord.shape[0], -1, np.int32),
+                   fun_npts=np.array([3], np.int32), fun_smooth=np.array([1], np.int32),
+                   fun_tab=tab, lmate=lmate, fext=fext, load_fun=0, dtime=dt, nsteps=nsteps,
+                   name=f"ensemble_{nspec}", info=dict(specimens=nspec, elements=int(lnods.shape[0]),
+                                                       sizes=[int(v) for v in np.bincount(lmate)]))
 
 
 def cantilever_400x40x40(nsteps=20000, seed=0, ref_equivalent=False, div=1):

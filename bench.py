@@ -35,7 +35,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "cantilever_400x40x40_hex08"
+WORKLOADS = {"cantilever": "cantilever_400x40x40_hex08",
+             "cylinder": "cylinder_ogrid_2.0M_hex08_per_element_materials",
+             "ensemble": "ensemble_256_specimens_hex08"}
 
 
 def parse():
@@ -50,6 +52,11 @@ def parse():
     ap.add_argument("--div", type=int, default=1, help="coarsen the mesh (tests only)")
     ap.add_argument("--prestrain", type=float, default=0.01,
                     help="initial axial strain (both arms): 1%% is just past the AS start")
+    ap.add_argument("--workload", default="cantilever", choices=list(WORKLOADS),
+                    help="cantilever 400x40x40 (default), cylinder (2.0M-element O-grid, per-element "
+                         "materials, temperature field) or ensemble (256 specimens)")
+    ap.add_argument("--block", type=int, default=0, help="threads per element block (0: library default)")
+    ap.add_argument("--autotune", action="store_true", help="pick block and scatter by timing candidates")
     return ap.parse_args()
 
 
@@ -139,8 +146,12 @@ def algorithmic_bytes(prob, precision):
     return prob.nelem * (32 + 2 * 8 * 3 * s) + prob.npoin * (24 + 24 + 48)
 
 
-def build_problem(div):
+def build_problem(workload, div):
     from alya_sma_b200 import problem as P
+    if workload == "cylinder":
+        return P.cylinder_2m(nsteps=10000, div=div)
+    if workload == "ensemble":
+        return P.ensemble(nspec=max(2, 256 // div), nsteps=5000)
     return P.cantilever_400x40x40(nsteps=20000, div=div)
 
 
@@ -170,14 +181,14 @@ def run_reference(args):
     if world > 1 and rank != 0:
         return 0
     from alya_sma_b200 import problem as P
-    prob = build_problem(args.div)
+    prob = build_problem(args.workload, args.div)
     u0 = P.prestrain(prob, args.prestrain)
     base = cpu_baseline(prob, u0, budget_s=15.0, max_steps=max(2, args.steps))
     line = {"impl": "reference", "metric": "Gauss-point updates/s (explicit SMA step)",
             "value": base["value"], "unit": "GP-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nelem": prob.nelem, "npoin": prob.npoin,
+            "config": {"workload": WORKLOADS[args.workload], "nelem": prob.nelem, "npoin": prob.npoin,
                        "gauss_points": prob.nelem * 8, "precision": "fp64 (reference CPU path)",
                        "prestrain": args.prestrain},
             "cpu_baseline": base,
@@ -199,12 +210,21 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    prob = build_problem(args.div)
+    prob = build_problem(args.workload, args.div)
     nelem, ngp = prob.nelem, prob.nelem * 8
 
     from alya_sma_b200 import problem as P
     u0 = P.prestrain(prob, args.prestrain)
-    solid = sma.ExplicitSolid(prob, precision=args.precision, scatter=args.scatter, device=local)
+    block, scatter, tuned = args.block, args.scatter, None
+    if args.autotune:
+        from alya_sma_b200 import tune
+        tuned = tune.tune(prob, precision=args.precision, displ=u0, steps=10, warmup=3, device=local)
+        block, scatter, variant = tuned["block"], tuned["scatter"], tuned["variant"]
+    else:
+        variant = "auto"
+    args.scatter = scatter
+    solid = sma.ExplicitSolid(prob, precision=args.precision, scatter=scatter, block=block,
+                              device=local, variant=variant)
     solid.set("displ", u0)
     stream = torch.cuda.ExternalStream(solid.stream)
     solid.step(max(3, args.warmup))
@@ -303,9 +323,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if args.precision == "fp32" else "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "nelem": nelem, "npoin": prob.npoin,
+                "config": {"workload": WORKLOADS[args.workload], "nelem": nelem, "npoin": prob.npoin,
                            "gauss_points": ngp, "precision": args.precision,
-                           "scatter": args.scatter, "dtime": prob.dtime,
+                           "scatter": args.scatter, "block": block or (256 if args.precision == "fp32" else 128), "variant": variant, "autotuned": bool(tuned), "dtime": prob.dtime,
                            "prestrain": args.prestrain,
                            "l2": "working set > L2 (state, nodal arrays and connectivity "
                                  f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",

@@ -95,7 +95,19 @@ typedef struct {
   const double*  fext;      /* (3, npoin) nodal load at load factor 1, or NULL */
   int32_t load_fun;         /* table whose vx column scales fext, or -1        */
   int32_t block;            /* threads per element-kernel block (0 = tuned)    */
+  int32_t scheme;           /* SMA_SCHEME_CD or SMA_SCHEME_TW                   */
+  double  phitw;            /* Tchamwa-Wielgosz phi (0: the reference's 1.033) */
+  int32_t variant;          /* element kernel: SMA_VARIANT_*                   */
 } sma_run_desc;
+
+/* element-loop kernels */
+#define SMA_VARIANT_AUTO    0   /* FP32: PIPE, FP64: PLAIN (measured on B200)                 */
+#define SMA_VARIANT_PIPE    1   /* persistent blocks, next tile's gather in flight (cp.async) */
+#define SMA_VARIANT_PLAIN   2   /* one tile per block                                        */
+
+/* explicit schemes (TIME_INTEGRATION of sld_reanut.f90:118-184) */
+#define SMA_SCHEME_CD       0   /* central difference, mod_sld_solution_methods.f90:101-223 */
+#define SMA_SCHEME_TW       1   /* Tchamwa-Wielgosz, mod_sld_solution_methods.f90:385-574   */
 
 typedef struct { int64_t c[SMA_NCOUNTERS]; double gpdet_min; } sma_counters;
 
@@ -168,11 +180,28 @@ int32_t sma_get_time(sma_ctx* ctx, double* cutim);
 int32_t sma_set_time(sma_ctx* ctx, double cutim);
 int32_t sma_get_counters(sma_ctx* ctx, sma_counters* out);
 int32_t sma_reset_counters(sma_ctx* ctx);
-/* witness dofs (flat ids 3*p+i): their displacement after each step of the
- * next sma_explicit_step call is recorded on the device; sma_get_witness
- * copies (nsteps, nwit) values of the last call. */
+/* witness dofs: flat ids 3*p+i record the displacement of dof i of node p
+ * after each step of the next sma_explicit_step call, ids 3*npoin + 3*p+i
+ * its residual (f_ext - f_int; on prescribed dofs the reaction, as
+ * frxid_sld); sma_get_witness copies (nsteps, nwit) values of the last call. */
 int32_t sma_set_witness(sma_ctx* ctx, int32_t nwit, const int32_t* dofs, int32_t max_steps);
 int32_t sma_get_witness(sma_ctx* ctx, double* host, int32_t* nsteps_out);
+
+/* Energy balance of sld_energy (mod_sld_energy.f90:71-193), accumulated on
+ * the device after every step while enabled: totals[5] = ALLIE (internal
+ * work), ALLWK (external work), ALLKE (kinetic energy), ETOTA = ALLIE + ALLKE
+ * - ALLWK, EENER.  Enabling records one row of the five per step of the next
+ * sma_explicit_step calls (up to max_steps rows; sma_get_energy returns them
+ * and the current totals).  Body forces are not part of the balance. */
+int32_t sma_set_energy(sma_ctx* ctx, int32_t enable, int32_t max_steps);
+int32_t sma_get_energy(sma_ctx* ctx, double* totals, double* hist, int32_t* nrows);
+
+/* Checkpoint of the step-boundary state (the restart data of
+ * mod_sld_arrays.f90:61-73: displacement, velocity, acceleration, svegm, and
+ * the time), in a binary file; loading it into a context of the same mesh
+ * and precision resumes bit for bit. */
+int32_t sma_checkpoint_save(sma_ctx* ctx, const char* path);
+int32_t sma_checkpoint_load(sma_ctx* ctx, const char* path);
 
 /* critical time step of the mesh (mod_sld_minle_time_step.f90:262-268) */
 int32_t sma_critical_dt(sma_ctx* ctx, double* dtcri);

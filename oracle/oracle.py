@@ -204,11 +204,14 @@ class Problem:
     def critical_dt(self):
         return critical_dt(self.lnods, self.coord, self.props, self.densi, self.lmate, self.dtype)
 
-    def run(self, dtime, nsteps, wit_dof=None):
-        """Central-difference time loop; returns the witness history
-        (nsteps, nwit) of displ at flat dof ids 3*ipoin+idime."""
+    def run(self, dtime, nsteps, wit_dof=None, scheme="cd", phi=1.033):
+        """Explicit time loop (scheme "cd" central difference or "tw"
+        Tchamwa-Wielgosz); returns the witness history (nsteps, nwit) of displ
+        at flat dof ids 3*ipoin+idime."""
         ct = self.ct
         wit = np.zeros(0, np.int32) if wit_dof is None else np.ascontiguousarray(wit_dof, np.int32)
+        if wit.size and (wit.min() < 0 or wit.max() >= 3 * self.npoin):
+            raise ValueError("oracle witnesses are displacement dofs in [0, 3*npoin)")
         hist = np.zeros((nsteps, max(1, wit.size)), self.dtype)
         fn = getattr(lib(), "orc_run_cd" + self.sfx)
         fn.argtypes = None
@@ -221,5 +224,5 @@ class Problem:
            _ptr(self.color_elem, C.c_int32), self.nthreads, ct(dtime), int(nsteps),
            _ptr(self.cutim, ct), _ptr(self.displ, ct), _ptr(self.veloc, ct), _ptr(self.accel, ct),
            _ptr(self.sdv, ct), _ptr(self.rhsid, ct), int(wit.size), _ptr(wit, C.c_int32),
-           _ptr(hist, ct), _ptr(self.counters, C.c_int32))
+           _ptr(hist, ct), _ptr(self.counters, C.c_int32), 1 if scheme == "tw" else 0, ct(phi))
         return hist[:, : wit.size]

@@ -85,7 +85,8 @@ extern "C" {
                      const int32_t* color_ptr, const int32_t* color_elem,           \
                      int nthreads, T dtime, int nsteps, T* cutim, T* displ,         \
                      T* veloc, T* accel, T* sdv, T* rhsid, int nwit,                \
-                     const int32_t* wit_dof, T* wit_hist, int32_t* counters);
+                     const int32_t* wit_dof, T* wit_hist, int32_t* counters,        \
+                     int scheme, T phi);
 
 ORC_DECL(double, _f64)
 ORC_DECL(float, _f32)

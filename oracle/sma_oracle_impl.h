@@ -714,7 +714,8 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
                    const int32_t* color_ptr, const int32_t* color_elem,
                    int nthreads, REAL dtime, int nsteps, REAL* cutim, REAL* displ,
                    REAL* veloc, REAL* accel, REAL* sdv, REAL* rhsid, int nwit,
-                   const int32_t* wit_dof, REAL* wit_hist, int32_t* counters)
+                   const int32_t* wit_dof, REAL* wit_hist, int32_t* counters,
+                   int scheme, REAL phi)
 {
   int64_t ndof = 3 * (int64_t)npoin;
   REAL* vtmp = (REAL*)malloc(sizeof(REAL) * ndof);
@@ -732,8 +733,15 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
     for (int p = 0; p < npoin; ++p)
       for (int i = 0; i < 3; ++i) {
         int64_t k = i + 3 * (int64_t)p;
-        vtmp[k] = veloc[k] + c_pred * accel[k];
-        REAL u = displ[k] + dtime * vtmp[k];
+        REAL u;
+        if (scheme == 1) {
+          /* Tchamwa-Wielgosz predictor, mod_sld_solution_methods.f90:406-417 */
+          vtmp[k] = veloc[k] + dtime * accel[k];
+          u = displ[k] + dtime * veloc[k] + phi * (dtime * dtime) * accel[k];
+        } else {
+          vtmp[k] = veloc[k] + c_pred * accel[k];
+          u = displ[k] + dtime * vtmp[k];
+        }
         if (fixno[k] == 1) {
           int f = bcfun ? bcfun[p] : -1;
           u = (f >= 0) ? FN(orc_funbou)(fun_npts[f], fun_tab + fun_off[f], fun_smooth[f], i, *cutim)
@@ -757,8 +765,14 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
       for (int i = 0; i < 3; ++i) {
         int64_t k = i + 3 * (int64_t)p;
         REAL a = (REAL)0 + rhsid[k] * fact1;
-        accel[k] = a;
-        veloc[k] = vtmp[k] + c_corr * a;
+        if (scheme == 1) {
+          /* TW corrector, :504-515: prescribed dofs at rest */
+          if (fixno[k] == 1) { accel[k] = 0; veloc[k] = 0; }
+          else { accel[k] = a; veloc[k] = vtmp[k]; }
+        } else {
+          accel[k] = a;
+          veloc[k] = vtmp[k] + c_corr * a;
+        }
         if (!(a == a) || a - a != 0) nonfin++;
       }
     }

@@ -1,0 +1,87 @@
+"""Workload paths of the north-star configurations at oracle-sized
+resolution: per-element materials and a temperature field (the O-grid
+cylinder), the batched ensemble, and the autotuner."""
+import numpy as np
+import pytest
+
+import alya_sma_b200 as sma
+from alya_sma_b200 import problem as P
+from alya_sma_b200 import tune
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+
+
+def _traj(oracle, p, nsteps, wit, precision="fp64", **kw):
+    o = oracle.Problem(p)
+    h_ref = o.run(p.dtime, nsteps, wit_dof=wit)
+    g = sma.ExplicitSolid(p, precision=precision, **kw)
+    g.set_witness(wit, nsteps)
+    g.step(nsteps)
+    return o, g, h_ref, g.witness()
+
+
+def test_cylinder_per_element_materials_and_temperature(oracle):
+    p = P.cylinder_2m(nsteps=600, div=8)
+    assert p.nelem == 3904 and len(p.props) == p.nelem
+    mid = int(np.argmin(np.sum((p.coord - [25.0, 0.0, 2.0]) ** 2, axis=1)))
+    q = int(np.argmin(np.sum((p.coord - [40.0, 4.0, 0.0]) ** 2, axis=1)))
+    wit = [3 * mid, 3 * mid + 1, 3 * mid + 2, 3 * q, 3 * q + 1]
+    o, g, h_ref, h = _traj(oracle, p, 300, wit)
+    scale = np.abs(h_ref).max(axis=0)
+    assert np.all(np.abs(h - h_ref).max(axis=0) <= 1e-6 * scale)
+    # reactions on the pushed face equal the oracle's residual there
+    tip = P.face_nodes(p.coord, 0, 50.0)
+    r = g.get("rhsid")[tip, 0]
+    assert np.abs(r - o.rhsid[tip, 0]).max() <= 1e-6 * np.abs(o.rhsid[tip, 0]).max()
+    xs, xs_ref = g.state[:, 1, :, 0], o.sdv[:, 1, :, 0]
+    assert np.abs(xs - xs_ref).max() < 1e-5
+    assert g.counters()["nr_active"] > 0
+
+
+def test_ensemble_matches_oracle_and_isolated_specimens(oracle):
+    p = P.ensemble(nspec=6, nsteps=400, emin=100, emax=400)
+    sizes = p.info["sizes"]
+    wit = []
+    node0 = 0
+    for s in range(6):                                   # tip x-displacement of each specimen
+        nn = int(np.sum(p.lmate == s))
+        wit.append(3 * int(np.argmax(np.where(np.isin(np.arange(p.npoin), np.unique(p.lnods[p.lmate == s])),
+                                              p.coord[:, 0], -1.0))))
+    o, g, h_ref, h = _traj(oracle, p, 200, wit)
+    assert np.abs(h - h_ref).max() <= 1e-6 * np.abs(h_ref).max()
+    assert np.all(np.abs(h_ref[-1]) > 0)
+    # specimen 0 alone, same dt: identical to its part of the ensemble
+    e0 = p.lmate == 0
+    nodes = np.unique(p.lnods[e0])
+    remap = -np.ones(p.npoin, np.int64)
+    remap[nodes] = np.arange(nodes.size)
+    q = P.Problem(coord=p.coord[nodes], lnods=remap[p.lnods[e0]].astype(np.int32), props=p.props[:1],
+                  e_mart=p.e_mart[:1], densi=p.densi[:1], fixno=p.fixno[nodes], bcfun=p.bcfun[nodes],
+                  fun_npts=p.fun_npts, fun_smooth=p.fun_smooth, fun_tab=p.fun_tab, fext=p.fext[nodes],
+                  load_fun=p.load_fun, dtime=p.dtime, nsteps=p.nsteps)
+    g1 = sma.ExplicitSolid(q, precision="fp64")
+    g1.step(200)
+    u_all = g.get("displ")[nodes]
+    u_one = g1.get("displ")
+    assert np.abs(u_all - u_one).max() <= 1e-12 * np.abs(u_one).max()
+
+
+def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
+    monkeypatch.setenv("ALYA_SMA_CACHE", str(tmp_path))
+    p = P.ensemble(nspec=4, nsteps=100, emin=200, emax=800)
+    r = tune.tune(p, precision="fp32", steps=5, warmup=2)
+    assert (r["block"], r["scatter"], r["variant"]) in list(tune.CANDIDATES)
+    assert len(r["trials"]) == len(tune.CANDIDATES)
+    assert all(t["step_ms"] > 0 for t in r["trials"].values())
+    again = tune.tune(p, precision="fp32", steps=5, warmup=2)
+    assert again == r                                   # served from the cache
+    s = tune.autotuned(p, precision="fp32", steps=5, warmup=2)
+    s.step(10)
+    assert s.counters()["nonfinite"] == 0
