@@ -372,7 +372,16 @@ def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0)
                    info=dict(mesh=f"O-grid core {nc}x{nc}, ring {nr}, {nx} layers", elements=ne))
 
 
-def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15):
+def ensemble_sizes(nspec=256, seed=0, emin=1000, emax=50000):
+    """Element counts of the ensemble's specimens (10 k^3 for k = round((n/10)^(1/3)),
+    n drawn log-uniform in [emin, emax])."""
+    rng = np.random.default_rng(seed)
+    n_target = np.exp(rng.uniform(np.log(emin), np.log(emax), size=nspec))
+    k = np.maximum(2, np.round((n_target / 10.0) ** (1.0 / 3.0)).astype(int))
+    return 10 * k ** 3
+
+
+def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15, subset=None):
     """Batched ensemble: nspec independent NiTi specimens (10:1:1 bars, 1 mm
     elements) with element counts drawn log-uniform in [emin, emax] and every
     specimen's E_A, E_M, eps_L and transformation stresses scaled by
@@ -380,14 +389,18 @@ def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15)
     node ranges), so one element launch and one step graph cover all of them.
     Each is clamped at its x = 0 face and pulled by an axial tip traction of
     its own amplitude (0.8 to 1.5 times its forward-finish stress) through a
-    shared smooth load cycle; one dt (0.5 dt_crit of the stiffest specimen)."""
-    rng = np.random.default_rng(seed)
-    n_target = np.exp(rng.uniform(np.log(emin), np.log(emax), size=nspec))
+    shared smooth load cycle; one dt (0.5 dt_crit of the stiffest specimen).
+    `subset` (specimen ids) builds only those specimens -- each specimen's
+    random numbers come from its own stream, so a subset is identical to the
+    same specimens of the full ensemble (used to shard across GPUs)."""
+    sizes = ensemble_sizes(nspec, seed, emin, emax)
+    ids = list(range(nspec)) if subset is None else [int(v) for v in subset]
     coords, lnods_l, props_l, em_l, fixno_l, fext_l, spec_of = [], [], [], [], [], [], []
     off = 0
     base = nitinol_props(**NITI)
-    for s in range(nspec):
-        k = max(2, int(round((n_target[s] / 10.0) ** (1.0 / 3.0))))
+    for local, s in enumerate(ids):
+        rng = np.random.default_rng((seed, s))
+        k = int(round((sizes[s] / 10) ** (1.0 / 3.0)))
         nx, ny = 10 * k, k
         c, l = structured_box(nx, ny, ny, float(nx), float(ny), float(ny), 0.05, seed + 100 + s)
         f = rng.uniform(1.0 - spread, 1.0 + spread, size=7)
@@ -403,14 +416,14 @@ def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15)
         lnods_l.append(l + off)
         fixno_l.append(fx)
         fext_l.append(fe)
-        spec_of.append(np.full(l.shape[0], s, np.int32))
+        spec_of.append(np.full(l.shape[0], local, np.int32))
         off += c.shape[0]
     coord = np.concatenate(coords)
     lnods = np.concatenate(lnods_l).astype(np.int32)
     lmate = np.concatenate(spec_of)
     props = np.array(props_l)
     e_mart = np.array(em_l)
-    densi = np.full(nspec, NITI_DENSITY)
+    densi = np.full(len(ids), NITI_DENSITY)
     fixno = np.concatenate(fixno_l)
     fext = np.concatenate(fext_l)
     dt = 0.5 * critical_dt(coord, lnods, props, densi, lmate)
@@ -419,7 +432,8 @@ def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15)
                    fixno=fixno, bcfun=np.full(coord.shape[0], -1, np.int32),
                    fun_npts=np.array([3], np.int32), fun_smooth=np.array([1], np.int32),
                    fun_tab=tab, lmate=lmate, fext=fext, load_fun=0, dtime=dt, nsteps=nsteps,
-                   name=f"ensemble_{nspec}", info=dict(specimens=nspec, elements=int(lnods.shape[0]),
+                   name=f"ensemble_{nspec}", info=dict(specimens=len(ids), ids=ids,
+                                                       elements=int(lnods.shape[0]),
                                                        sizes=[int(v) for v in np.bincount(lmate)]))
 
 
