@@ -299,48 +299,67 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance) {
   return a;
 }
 
-// resident blocks per SM of a kernel at this block size and shared memory
-template <typename K>
-int32_t resident_blocks(K kernel, int block, size_t smem, int* out) {
-  CU(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, kernel, block, smem));
-  if (*out < 1) return fail(SMA_ERR_ARG, "element kernel does not fit on an SM at this block size");
-  return SMA_OK;
-}
-
 // kernel attributes and the persistent grid, fixed at context creation (not
 // inside a stream capture)
+// the element kernel of a variant, scatter and material layout
+template <typename T>
+using ElemKernel = void (*)(ElemArgs<T>);
+
+template <typename T, bool ATOMIC, bool MATS>
+ElemKernel<T> elem_kernel_v(bool pipe) {
+  return pipe ? k_element_pipe<T, ATOMIC, MATS> : k_element<T, ATOMIC, MATS>;
+}
+
+template <typename T>
+ElemKernel<T> elem_kernel(const sma_ctx* c) {
+  const bool pipe = c->variant == SMA_VARIANT_PIPE;
+  const bool atomic = c->scatter != SMA_SCATTER_COLOR;
+  const bool mats = c->d_lmate != nullptr;
+  if (atomic) return mats ? elem_kernel_v<T, true, true>(pipe) : elem_kernel_v<T, true, false>(pipe);
+  return mats ? elem_kernel_v<T, false, true>(pipe) : elem_kernel_v<T, false, false>(pipe);
+}
+
+template <typename T>
+size_t elem_smem(const sma_ctx* c) {
+  const bool mats = c->d_lmate != nullptr;
+  return c->variant == SMA_VARIANT_PIPE ? element_pipe_smem_bytes<T>(c->block, mats)
+                                        : element_smem_bytes<T>(c->block, mats);
+}
+
+// The kernel's dynamic shared-memory limit is a per-process attribute shared
+// by every context (and the no-alloc entry point): it is raised to what a
+// 256-thread block needs and never lowered.
 template <typename T>
 int32_t init_element_launch_t(sma_ctx* c) {
-  if (c->variant != SMA_VARIANT_PIPE) return SMA_OK;
-  const size_t smem = element_pipe_smem_bytes<T>(c->block);
-  return (c->scatter == SMA_SCATTER_COLOR)
-             ? resident_blocks(k_element_pipe<T, false>, c->block, smem, &c->resident)
-             : resident_blocks(k_element_pipe<T, true>, c->block, smem, &c->resident);
+  const int block = c->block;
+  c->block = 256;
+  const size_t smem256 = elem_smem<T>(c);
+  c->block = block;
+  const size_t smem = elem_smem<T>(c);
+  const ElemKernel<T> k = elem_kernel<T>(c);
+  CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)std::max<size_t>(smem256, 48 * 1024)));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->resident, k, block, smem));
+  if (c->resident < 1) return fail(SMA_ERR_ARG, "element kernel does not fit on an SM at this block size");
+  return SMA_OK;
 }
 
 template <typename T>
 int32_t launch_elements_t(sma_ctx* c, bool advance) {
   const int nrange = (int)c->cptr.size() - 1;
   const int epb = c->block / 8;
-  const bool color = c->scatter == SMA_SCATTER_COLOR;
-  if (c->variant == SMA_VARIANT_PIPE && c->resident == 0)
-    return fail(SMA_ERR_STATE, "element launch not initialised");
+  if (c->resident == 0) return fail(SMA_ERR_STATE, "element launch not initialised");
+  const ElemKernel<T> kern = elem_kernel<T>(c);
+  const size_t smem = elem_smem<T>(c);
   for (int r = 0; r < nrange; ++r) {
     const int beg = c->cptr[r], end = c->cptr[r + 1];
     if (end <= beg) continue;
     ElemArgs<T> a = elem_args<T>(c, beg, end, advance && r == 0);
     const int64_t ntiles = ceil_div(end - beg, epb);
-    if (c->variant == SMA_VARIANT_PIPE) {
-      const size_t smem = element_pipe_smem_bytes<T>(c->block);
-      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident);
-      if (color) k_element_pipe<T, false><<<grid, c->block, smem, c->stream>>>(a);
-      else k_element_pipe<T, true><<<grid, c->block, smem, c->stream>>>(a);
-    } else {
-      const size_t smem = element_smem_bytes<T>(c->block);
-      if (color) k_element<T, false><<<(unsigned)ntiles, c->block, smem, c->stream>>>(a);
-      else k_element<T, true><<<(unsigned)ntiles, c->block, smem, c->stream>>>(a);
-    }
+    const unsigned grid = c->variant == SMA_VARIANT_PIPE
+                              ? (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident)
+                              : (unsigned)ntiles;
+    kern<<<grid, c->block, smem, c->stream>>>(a);
     c->launches++;
   }
   CU(cudaGetLastError());
@@ -604,11 +623,12 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   TRYCU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   c->prec = run->precision;
   c->scatter = (run->scatter == SMA_SCATTER_COLOR) ? SMA_SCATTER_COLOR : SMA_SCATTER_ATOMIC;
-  // defaults measured on B200 (cantilever 640k elements, blocks 64..256):
-  // FP32 pipelined 256 threads; FP64 plain 128 threads (the pipelined FP64
-  // kernel needs ~200 registers and loses occupancy)
+  // defaults measured on B200 (cantilever 640k and cylinder 2.0M elements,
+  // fixed step windows): the one-tile kernel at 128 threads in both
+  // precisions; with the register caps of the element kernels the pipelined
+  // variant spills and is 10-50 % slower
   if (run->variant == SMA_VARIANT_AUTO)
-    c->variant = (c->prec == SMA_PREC_FP32) ? SMA_VARIANT_PIPE : SMA_VARIANT_PLAIN;
+    c->variant = SMA_VARIANT_PLAIN;
   else
     c->variant = (run->variant == SMA_VARIANT_PLAIN) ? SMA_VARIANT_PLAIN : SMA_VARIANT_PIPE;
   c->block = run->block ? run->block : ((c->variant == SMA_VARIANT_PIPE) ? 256 : 128);
@@ -1256,8 +1276,8 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   a.end = nelem;
   a.has_grav = 0;
   const int block = 256, epb = block / 8;
-  const size_t smem = element_smem_bytes<T>(block);
-  k_element<T, true><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
+  const size_t smem = element_smem_bytes<T>(block, false);      // below the 48 KB default
+  k_element<T, true, false><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
   k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
   CU(cudaGetLastError());
   return SMA_OK;
@@ -1287,6 +1307,10 @@ extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int3
     // set-up, once per device, with that device current
     void* p = nullptr;
     CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    CU(cudaFuncSetAttribute(k_element<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            48 * 1024));
+    CU(cudaFuncSetAttribute(k_element<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            48 * 1024));
     g_noalloc_ptr[dev] = (unsigned char*)p;
   }
   unsigned char* base = g_noalloc_ptr[dev];

@@ -184,22 +184,23 @@ __device__ __forceinline__ void lds8(const double* p, double* v) {
 // Work of one lane (element le, lane a) on one tile once its node is
 // gathered: dX, dU are node a's coordinates and displacement relative to the
 // element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
-// Gauss point a.  Stages the node rows, then phase 1 (lane = Gauss point),
-// the law, phase 2 (lane = node) and the scatter-add.  Needs the block's
-// reference table in `tab`.
+// Gauss point a, `mat` the element's material (the kernel parameter for a
+// one-material mesh, so its constants are instruction operands; a shared-
+// memory copy otherwise) and `tmp` its temperature.  Stages the node rows,
+// then phase 1 (lane = Gauss point), the law, phase 2 (lane = node) and the
+// scatter-add.  Needs the block's reference table in `tab`.
 template <typename T, bool ATOMIC>
 __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab, T* nsm, T* qsm,
                                              int lane8, bool valid, int64_t ec, int nid,
                                              const double* dX, const double* dU,
-                                             double xS, double F_AS, double F_SA) {
+                                             double xS, double F_AS, double F_SA,
+                                             const MatC& mat, double tmp) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     nsm[8 * c + lane8] = (T)dX[c];
     nsm[8 * (3 + c) + lane8] = (T)dU[c];
   }
   const int64_t gp = 8 * ec + lane8;
-  const int im = a.lmate ? a.lmate[ec] : 0;
-  const double tmp = a.tempe ? a.tempe[ec] : 0.0;
   __syncwarp();                                                  // node rows of the element
 
   // ---- phase 1, lane = Gauss point g: J = dX/dxi, Gu = du/dxi ------------
@@ -234,8 +235,6 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
       H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
 
   // ---- constitutive update ----------------------------------------------
-  // one material: constants come from the kernel parameters, no loads
-  const MatC& mat = a.lmate ? a.mats[im] : a.mat0;
   T tau[6];
   const int flag = law160_tau<T>(mat, H, tmp, xS, F_AS, F_SA, tau);
   if (valid) {
@@ -307,10 +306,33 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   count_warp(a.cnt, CNT_NEG_DET, valid && !(detF > T(0)));
 }
 
+// a material is copied as MAT_CHUNKS 16-byte chunks by the 8 lanes of its element
+constexpr int MAT_CHUNKS = (int)(sizeof(MatC) / 16);
+static_assert(sizeof(MatC) % 16 == 0 && MAT_CHUNKS <= 16, "MatC copy layout");
+
+// The element's material: the kernel parameter (one material) or the copy
+// in shared memory (per-element materials).
+template <bool MATS, typename T>
+__device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC* msm) {
+  if constexpr (MATS) return *msm;
+  else return a.mat0;
+}
+
+// Minimum resident blocks of 256 threads the element kernels are compiled
+// for, which caps their registers at 65536 / (256 x blocks).  Measured on
+// B200 over fixed step windows: the one-tile FP32 kernel with one material is
+// fastest at 3 (80 registers, 24 warps per SM, 20 bytes of spills); with
+// per-element materials, in the pipelined kernel and in FP64 the spills of
+// a tighter cap cost more than the extra warps gain, so 2 (128 registers).
+template <typename T, bool PIPE, bool MATS>
+constexpr int elem_min_blocks() { return (sizeof(T) == 4 && !PIPE && !MATS) ? 3 : 2; }
+
 // One tile of elements per block: each lane gathers its node with __ldg,
-// takes node 1's values from lane 0 of its element by shuffle.
-template <typename T, bool ATOMIC>
-__global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
+// takes node 1's values from lane 0 of its element by shuffle.  MATS: the
+// mesh has per-element materials (lmate), copied into shared memory per
+// element.
+template <typename T, bool ATOMIC, bool MATS>
+__global__ void __launch_bounds__(256, (elem_min_blocks<T, false, MATS>())) k_element(ElemArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tab = reinterpret_cast<T*>(smem_raw);                       // [8][8][4]
   T* elem_sm = tab + 256;
@@ -322,11 +344,19 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
   const int64_t ec = valid ? e : (int64_t)a.end - 1;
   T* nsm = elem_sm + le * ElemSmem<T>::PER_ELEM;                 // node rows [6][8]
   T* qsm = nsm + ElemSmem<T>::NODE_STRIDE;                       // Q rows [8][12]
+  MatC* msm = reinterpret_cast<MatC*>(elem_sm + epb * ElemSmem<T>::PER_ELEM) + le;
 
   if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
   fill_hex8_table<T>(tab);
 
   const int nid = a.lnods[8 * ec + lane8];
+  const double tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
+  if constexpr (MATS) {
+    const uint4* src = reinterpret_cast<const uint4*>(a.mats + __ldg(a.lmate + ec));
+    uint4* dst = reinterpret_cast<uint4*>(msm);
+    dst[lane8] = __ldg(src + lane8);
+    if (lane8 + 8 < MAT_CHUNKS) dst[8 + lane8] = __ldg(src + 8 + lane8);
+  }
   double X[3], U[3], dX[3], dU[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -342,8 +372,9 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
   const int64_t gp = 8 * ec + lane8;
   const double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp];
   const double F_SA = (double)a.sold[2 * a.sst + gp];
-  __syncthreads();                                               // reference table
-  element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA);
+  __syncthreads();                                               // reference table, materials
+  element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA,
+                          elem_mat<MATS>(a, msm), tmp);
 }
 
 // ---------------------------------------------------------------------------
@@ -355,22 +386,28 @@ __global__ void __launch_bounds__(256) k_element(ElemArgs<T> a) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+  if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+  else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-// one stage per element: 8 lanes x (X[3], U[3]) doubles, then 8 x 3 state T
-template <typename T>
+// one stage per element: 8 lanes x (X[3], U[3]) doubles, 8 x 3 state T
+// (padded to 4), the material (MATS) and the temperature (+ 8 bytes pad);
+// every part starts on a 16-byte boundary
+template <typename T, bool MATS>
 struct PipeStage {
   static constexpr int NODE_DOUBLES = 8 * 6;
-  static constexpr int BYTES = NODE_DOUBLES * 8 + 8 * 4 * sizeof(T);   // state padded to 4
+  static constexpr int MAT_OFF = NODE_DOUBLES * 8 + 8 * 4 * (int)sizeof(T);
+  static constexpr int TEMP_OFF = MAT_OFF + (MATS ? (int)sizeof(MatC) : 0);
+  static constexpr int BYTES = TEMP_OFF + 16;
 };
 
-template <typename T, bool ATOMIC>
-__global__ void __launch_bounds__(256) k_element_pipe(ElemArgs<T> a) {
+template <typename T, bool ATOMIC, bool MATS>
+__global__ void __launch_bounds__(256, (elem_min_blocks<T, true, MATS>())) k_element_pipe(ElemArgs<T> a) {
+  using PS = PipeStage<T, MATS>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tab = reinterpret_cast<T*>(smem_raw);
   T* elem_sm = tab + 256;
@@ -395,9 +432,9 @@ __global__ void __launch_bounds__(256) k_element_pipe(ElemArgs<T> a) {
     return v ? e : (int64_t)a.end - 1;
   };
   auto stage_ptr = [&](int s) -> unsigned char* {
-    return stages + ((size_t)s * epb + le) * PipeStage<T>::BYTES;
+    return stages + ((size_t)s * epb + le) * PS::BYTES;
   };
-  auto issue = [&](int s, int nid, int64_t ec) {
+  auto issue = [&](int s, int nid, int im, int64_t ec) {
     unsigned char* st = stage_ptr(s);
     double* nd = reinterpret_cast<double*>(st) + 6 * lane8;
 #pragma unroll
@@ -405,58 +442,73 @@ __global__ void __launch_bounds__(256) k_element_pipe(ElemArgs<T> a) {
       cp_async(nd + c, a.coord + c * a.npad + nid, 8);
       cp_async(nd + 3 + c, a.u + c * a.npad + nid, 8);
     }
-    T* ss = reinterpret_cast<T*>(st + PipeStage<T>::NODE_DOUBLES * 8) + 4 * lane8;
+    T* ss = reinterpret_cast<T*>(st + PS::NODE_DOUBLES * 8) + 4 * lane8;
     const int64_t gp = 8 * ec + lane8;
 #pragma unroll
     for (int c = 0; c < 3; ++c) cp_async(ss + c, a.sold + c * a.sst + gp, (int)sizeof(T));
+    if constexpr (MATS) {
+      const unsigned char* src = reinterpret_cast<const unsigned char*>(a.mats + im);
+      cp_async(st + PS::MAT_OFF + 16 * lane8, src + 16 * lane8, 16);
+      if (lane8 + 8 < MAT_CHUNKS)
+        cp_async(st + PS::MAT_OFF + 16 * (8 + lane8), src + 16 * (8 + lane8), 16);
+    }
+    if (a.tempe && lane8 == 0) cp_async(st + PS::TEMP_OFF, a.tempe + ec, 8);
   };
+  auto mate = [&](int64_t ec) -> int { return MATS ? a.lmate[ec] : 0; };
 
   bool v0, v1;
   int64_t ec0 = elem(t, v0);
   int nid0 = a.lnods[8 * ec0 + lane8];
-  issue(0, nid0, ec0);
+  issue(0, nid0, mate(ec0), ec0);
   cp_async_commit();
   int64_t t1 = t + gridDim.x;
   int64_t ec1 = elem(t1 < ntiles ? t1 : t, v1);
   int nid1 = a.lnods[8 * ec1 + lane8];
+  int im1 = mate(ec1);
   int s = 0;
   for (; t < ntiles; t += gridDim.x) {
     const int64_t tn = t + gridDim.x;
-    if (tn < ntiles) issue(s ^ 1, nid1, ec1);
+    if (tn < ntiles) issue(s ^ 1, nid1, im1, ec1);
     cp_async_commit();
     const int64_t tn2 = tn + gridDim.x;
     bool v2;
     const int64_t ec2 = elem(tn2 < ntiles ? tn2 : t, v2);
     const int nid2 = a.lnods[8 * ec2 + lane8];
+    const int im2 = mate(ec2);
     cp_async_wait1();                                            // this tile's copies landed
     __syncwarp();
     const unsigned char* st = stage_ptr(s);
     const double* nd = reinterpret_cast<const double*>(st);
-    const T* ss = reinterpret_cast<const T*>(st + PipeStage<T>::NODE_DOUBLES * 8) + 4 * lane8;
+    const T* ss = reinterpret_cast<const T*>(st + PS::NODE_DOUBLES * 8) + 4 * lane8;
     double dX[3], dU[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       dX[c] = nd[6 * lane8 + c] - nd[c];                         // relative to node 1 (lane 0)
       dU[c] = nd[6 * lane8 + 3 + c] - nd[3 + c];
     }
+    const double tmp = a.tempe ? *reinterpret_cast<const double*>(st + PS::TEMP_OFF) : 0.0;
     element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, v0, ec0, nid0, dX, dU, (double)ss[0],
-                            (double)ss[1], (double)ss[2]);
+                            (double)ss[1], (double)ss[2],
+                            elem_mat<MATS>(a, reinterpret_cast<const MatC*>(st + PS::MAT_OFF)), tmp);
     __syncwarp();                                                // stage s is reused next-but-one
     nid0 = nid1; ec0 = ec1; v0 = v1;
-    nid1 = nid2; ec1 = ec2; v1 = v2;
+    nid1 = nid2; ec1 = ec2; v1 = v2; im1 = im2;
     s ^= 1;
   }
   cp_async_wait0();
 }
 
 // dynamic shared memory of the element kernels for a block of `block` threads
+// (k_element: table, element rows, then one material per element if mats)
 template <typename T>
-inline size_t element_smem_bytes(int block) {
-  return (256 + (size_t)(block / 8) * ElemSmem<T>::PER_ELEM) * sizeof(T);
+inline size_t element_smem_bytes(int block, bool mats) {
+  return (256 + (size_t)(block / 8) * ElemSmem<T>::PER_ELEM) * sizeof(T) +
+         (mats ? (size_t)(block / 8) * sizeof(MatC) : 0);
 }
 template <typename T>
-inline size_t element_pipe_smem_bytes(int block) {
-  return element_smem_bytes<T>(block) + 2 * (size_t)(block / 8) * PipeStage<T>::BYTES;
+inline size_t element_pipe_smem_bytes(int block, bool mats) {
+  const size_t stage = mats ? PipeStage<T, true>::BYTES : PipeStage<T, false>::BYTES;
+  return element_smem_bytes<T>(block, false) + 2 * (size_t)(block / 8) * stage;
 }
 
 // ---------------------------------------------------------------------------

@@ -138,6 +138,17 @@ def profiled_traffic(precision):
         return None
 
 
+def profiled_issue(precision):
+    """Warp instructions per element-kernel launch from the same ncu summary
+    (line 'warp_inst_per_launch: N'); the B200 has 148 SMs."""
+    path = os.path.join(ROOT, "profiles", f"k_element_{precision}_cantilever.md")
+    try:
+        m = re.search(r"warp_inst_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        return {"warp_inst": float(m.group(1)), "sms": 148} if m else None
+    except OSError:
+        return None
+
+
 def algorithmic_bytes(prob, precision):
     """Minimum HBM traffic of one element-kernel launch: connectivity, state
     read + write, one read of coordinates and displacements and one
@@ -234,6 +245,13 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    # the state at the start of the timed region, to replay the same window
+    # with per-launch events (the element work depends on how many Gauss
+    # points transform, so a different window would time different work)
+    import tempfile
+    ckpt = os.path.join(tempfile.mkdtemp(prefix="sma_bench_"), f"window_r{rank}.bin")
+    solid.save(ckpt)
+
     # ---- timed region: K device-resident steps (CUDA graphs) ---------------
     clocks = Clocks(local)
     barrier()
@@ -254,9 +272,14 @@ def main():
         ms = float(t.item())
     value = world * ngp * args.steps / (ms / 1e3)
 
-    # ---- per-kernel device times (roofline of the element kernel) ---------
+    # ---- per-kernel device times (roofline of the element kernel): the same
+    # K steps replayed from the checkpoint, CUDA events around every launch
+    # on the library's stream ------------------------------------------------
+    solid.load(ckpt)
+    os.remove(ckpt)
+    os.rmdir(os.path.dirname(ckpt))
     solid.set_timing(True)
-    solid.step(min(args.steps, 60))
+    solid.step(args.steps)
     tm = solid.timers()
     solid.set_timing(False)
     el_ms = tm["element"][0] / max(1, tm["element"][1])
@@ -270,7 +293,19 @@ def main():
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg, "launch_ms": round(el_ms, 4),
                 "nodal_launch_ms": round(nd_ms, 4),
+                "window": "the K timed steps replayed from a checkpoint of their start, "
+                          "CUDA events around each launch on the library stream",
                 "note": "compute-bound kernel: the FP32/FP64 pipes, not HBM, bind it"}
+    issue = profiled_issue(args.precision)
+    if issue:
+        # instruction-issue roofline: warp instructions per launch (ncu) over
+        # the measured launch time, against 4 issue slots per SM per clock
+        rate = issue["warp_inst"] / (el_ms / 1e3)
+        peak_i = 4 * issue["sms"] * ck.get("sm_mhz", 1965.0) * 1e6
+        roofline["issue"] = {"warp_inst_per_launch": issue["warp_inst"],
+                             "achieved_ginst_s": round(rate / 1e9, 1),
+                             "peak_ginst_s": round(peak_i / 1e9, 1),
+                             "frac": round(rate / peak_i, 4)}
 
     extras = {}
     if not args.no_extras and rank == 0:
