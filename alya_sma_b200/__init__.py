@@ -94,6 +94,7 @@ def lib():
         L.sma_assemble.argtypes = [C.c_void_p, C.c_void_p, C.c_double] + [C.c_void_p] * 5
         L.sma_assemble_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
         L.sma_end_step.argtypes = [C.c_void_p]
+        L.sma_postprocess.argtypes = [C.c_void_p] * 6
         L.sma_eval_law160.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p]
@@ -196,6 +197,21 @@ class ExplicitSolid:
 
     def end_step(self):
         _check(lib().sma_end_step(self._ctx))
+
+    def postprocess(self, gp_sigma=False):
+        """sld_calculate_pp_tensors: nodal Cauchy stress 'caust', Green strain
+        'green' and log strain 'lepsi' as (npoin, 6) in Voigt order xx yy zz
+        yz xz xy, von Mises 'seqvm' (npoin,), and with gp_sigma the Cauchy
+        stress per Gauss point (nelem, 8, 6).  Evaluated at the current
+        displacement from the state the last element loop started from."""
+        out = {k: np.zeros((self.npoin, 6)) for k in ("caust", "green", "lepsi")}
+        out["seqvm"] = np.zeros(self.npoin)
+        gp = np.zeros((self.nelem, 8, 6)) if gp_sigma else None
+        _check(lib().sma_postprocess(self._ctx, _p(out["caust"]), _p(out["green"]), _p(out["lepsi"]),
+                                     _p(out["seqvm"]), _p(gp)))
+        if gp_sigma:
+            out["gp_sigma"] = gp
+        return out
 
     # -- data ----------------------------------------------------------------
     def get(self, field):

@@ -230,6 +230,10 @@ struct sma_ctx {
   MatC mat0;                               // material 0, passed by value when nmate == 1
   void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
   int cur = 0;                             // state buffer holding TIME_N
+  int last_in = -1;                        // state buffer the last element loop read (-1: none)
+  double* d_pp_acc = nullptr;              // post-processing: [19][npad] nodal sums
+  double* d_pp_out = nullptr;              //   (19, npoin) nodal results
+  double* d_pp_gp = nullptr;               //   (6, 8, nelem) Gauss-point Cauchy stress
   unsigned long long* d_cnt = nullptr;
   StepTime* d_ts = nullptr;
   FunTab* d_ft = nullptr;
@@ -349,6 +353,7 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
   const int nrange = (int)c->cptr.size() - 1;
   const int epb = c->block / 8;
   if (c->resident == 0) return fail(SMA_ERR_STATE, "element launch not initialised");
+  c->last_in = c->cur;
   const ElemKernel<T> kern = elem_kernel<T>(c);
   const size_t smem = elem_smem<T>(c);
   for (int r = 0; r < nrange; ++r) {
@@ -369,6 +374,27 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
 int32_t launch_elements(sma_ctx* c, bool advance) {
   return c->prec == SMA_PREC_FP32 ? launch_elements_t<float>(c, advance)
                                   : launch_elements_t<double>(c, advance);
+}
+
+// post-processing element pass reading state buffer `slot`
+template <typename T>
+int32_t launch_postproc_t(sma_ctx* c, int slot) {
+  ElemArgs<T> a = elem_args<T>(c, 0, c->nelem, false);
+  a.sold = (const T*)c->d_state[slot];
+  a.snew = nullptr;
+  PostArgs p;
+  p.acc = c->d_pp_acc;
+  p.gp_sig = c->d_pp_gp;
+  p.perm = c->d_perm;
+  const int block = 128;
+  const bool mats = c->d_lmate != nullptr;
+  const size_t smem = postproc_smem_bytes<T>(block, mats);      // below the 48 KB default
+  const unsigned grid = (unsigned)ceil_div(c->nelem, block / 8);
+  if (mats) k_postproc<T, true><<<grid, block, smem, c->stream>>>(a, p);
+  else k_postproc<T, false><<<grid, block, smem, c->stream>>>(a, p);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
 }
 
 NodalArgs nodal_args(sma_ctx* c) {
@@ -547,7 +573,8 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
                   c->d_f, c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
-                  c->d_fextp, c->d_en, c->d_ehist, c->d_erow, c->d_epart};
+                  c->d_fextp, c->d_en, c->d_ehist, c->d_erow, c->d_epart, c->d_pp_acc,
+                  c->d_pp_out, c->d_pp_gp};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -849,6 +876,42 @@ int32_t sma_end_step(sma_ctx* c) {
   return SMA_OK;
 }
 
+int32_t sma_postprocess(sma_ctx* c, double* caust, double* green, double* lepsi, double* seqvm,
+                        double* gp_sigma) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc;
+  if (!c->d_pp_acc && (rc = dalloc(&c->d_pp_acc, PP_COLS * (size_t)c->npad * sizeof(double)))) return rc;
+  if (!c->d_pp_out && (rc = dalloc(&c->d_pp_out, PP_COLS * (size_t)c->npoin * sizeof(double)))) return rc;
+  if (gp_sigma && !c->d_pp_gp && (rc = dalloc(&c->d_pp_gp, 48 * (size_t)c->nelem * sizeof(double))))
+    return rc;
+  double* gp_keep = c->d_pp_gp;
+  if (!gp_sigma) c->d_pp_gp = nullptr;                          // the kernel skips the per-GP output
+  const int slot = c->last_in >= 0 ? c->last_in : c->cur;
+  CU(cudaMemsetAsync(c->d_pp_acc, 0, PP_COLS * (size_t)c->npad * sizeof(double), c->stream));
+  rc = c->prec == SMA_PREC_FP32 ? launch_postproc_t<float>(c, slot) : launch_postproc_t<double>(c, slot);
+  c->d_pp_gp = gp_keep;
+  if (rc) return rc;
+  k_postproc_nodal<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(c->d_pp_acc, c->npad,
+                                                                             c->npoin, c->d_pp_out);
+  c->launches++;
+  CU(cudaGetLastError());
+  const size_t n6 = 6 * (size_t)c->npoin;
+  double* outs[3] = {caust, green, lepsi};
+  for (int t = 0; t < 3; ++t)
+    if (outs[t])
+      CU(cudaMemcpyAsync(outs[t], c->d_pp_out + t * n6, n6 * sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+  if (seqvm)
+    CU(cudaMemcpyAsync(seqvm, c->d_pp_out + 3 * n6, c->npoin * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+  if (gp_sigma)
+    CU(cudaMemcpyAsync(gp_sigma, c->d_pp_gp, 48 * (size_t)c->nelem * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
 int32_t sma_set_nodal(sma_ctx* c, int32_t field, const double* host) {
   if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
   double* dst = nullptr;
@@ -905,6 +968,7 @@ static int32_t state_io(sma_ctx* c, double* host, bool in) {
   void* sn = c->d_state[c->cur];
   cudaError_t e = cudaSuccess;
   if (in) {
+    c->last_in = -1;                       // post-processing reads TIME_N until the next loop
     e = cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
       if (c->prec == SMA_PREC_FP32)

@@ -181,6 +181,42 @@ __device__ __forceinline__ void lds8(const double* p, double* v) {
   }
 }
 
+// Phase 1 of a tile, lane = Gauss point g: J = dX/dxi and Gu = du/dxi from
+// the element's node rows in shared memory (relative to node 1, so node 1
+// drops out), Ji = J^-1 (Ji[3j+k] = dxi_j/dX_k) and H = dU/dX = Gu Ji
+// (jacobi.f90:172-219, sld_elmpre.f90:149-162).  Returns det J.
+template <typename T>
+__device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H) {
+  T J[9], Gu[9];
+  {
+    // this lane's Gauss point: derivatives in registers (a table row per
+    // lane would put the 8 lanes of an element in one shared-memory bank)
+    T N[8], dN[24];
+    hex8_gp<T>(g, N, dN);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { J[k] = T(0); Gu[k] = T(0); }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      T v[8];
+      lds8(nsm + 8 * c, v);
+#pragma unroll
+      for (int n = 1; n < 8; ++n) {
+        T* acc = (c < 3) ? J + 3 * c : Gu + 3 * (c - 3);
+        acc[0] += v[n] * dN[3 * n + 0];
+        acc[1] += v[n] * dN[3 * n + 1];
+        acc[2] += v[n] * dN[3 * n + 2];
+      }
+    }
+  }
+  const T detJ = inv3(J, Ji);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
+  return detJ;
+}
+
 // Work of one lane (element le, lane a) on one tile once its node is
 // gathered: dX, dU are node a's coordinates and displacement relative to the
 // element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
@@ -203,36 +239,9 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   const int64_t gp = 8 * ec + lane8;
   __syncwarp();                                                  // node rows of the element
 
-  // ---- phase 1, lane = Gauss point g: J = dX/dxi, Gu = du/dxi ------------
-  T J[9], Gu[9];
-  {
-    // this lane's Gauss point: derivatives in registers (a table row per
-    // lane would put the 8 lanes of an element in one shared-memory bank)
-    T N[8], dN[24];
-    hex8_gp<T>(lane8, N, dN);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) { J[k] = T(0); Gu[k] = T(0); }
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      T v[8];
-      lds8(nsm + 8 * c, v);
-#pragma unroll
-      for (int n = 1; n < 8; ++n) {
-        T* acc = (c < 3) ? J + 3 * c : Gu + 3 * (c - 3);
-        acc[0] += v[n] * dN[3 * n + 0];
-        acc[1] += v[n] * dN[3 * n + 1];
-        acc[2] += v[n] * dN[3 * n + 2];
-      }
-    }
-  }
-  T Ji[9];
-  const T detJ = inv3(J, Ji);                                    // Ji[3j+k] = dxi_j/dX_k
-  T H[9];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
+  // ---- phase 1, lane = Gauss point g ------------------------------------
+  T Ji[9], H[9];
+  const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H);
 
   // ---- constitutive update ----------------------------------------------
   T tau[6];
@@ -509,6 +518,160 @@ template <typename T>
 inline size_t element_pipe_smem_bytes(int block, bool mats) {
   const size_t stage = mats ? PipeStage<T, true>::BYTES : PipeStage<T, false>::BYTES;
   return element_smem_bytes<T>(block, false) + 2 * (size_t)(block / 8) * stage;
+}
+
+// ---------------------------------------------------------------------------
+// Stress/strain post-processing (sld_calculate_pp_tensors_ielem.f90:100-150,
+// 180-218; itask 3 of the element loop).  Lane = Gauss point: the law is
+// evaluated from the state in a.sold (its new state is discarded), then
+//   sigma = tau / det F                  (= F P^T / det F of the reference)
+//   E     = (H + H^T + H^T H) / 2        (Green strain, = (F^T F - I) / 2)
+//   lnV   = log1p(H + H^T + H H^T) / 2   (logarithmic strain)
+// and row g = dV_g (sigma, E, lnV, 1) in Voigt order xx yy zz yz xz xy
+// (nvgij_sld, sld_inivar.f90:568-579).  Lane = node a then adds
+// sum_g N_a(g) row_g into acc[19][npad] with FP64 atomics (the last column is
+// the volume-lumped mass of mod_mass_matrix.f90:150-215).  gp_sig, if not
+// null, receives sigma per Gauss point as (6, 8, nelem) in the caller's
+// element order (perm maps the internal order to it).
+// ---------------------------------------------------------------------------
+constexpr int PP_COLS = 19;
+constexpr int PP_ROW = 20;                 // doubles per Gauss-point row (16-byte multiple)
+
+struct PostArgs {
+  double* acc;                             // [PP_COLS][npad]
+  double* gp_sig;                          // (6, 8, nelem) or null
+  const int32_t* perm;                     // internal element -> caller's element
+};
+
+// shared memory: table, Gauss-point rows, node rows, materials
+template <typename T>
+inline size_t postproc_smem_bytes(int block, bool mats) {
+  const size_t epb = (size_t)(block / 8);
+  return 256 * sizeof(T) + epb * (8 * PP_ROW * sizeof(double) + ElemSmem<T>::NODE_STRIDE * sizeof(T)) +
+         (mats ? epb * sizeof(MatC) : 0);
+}
+
+template <typename T, bool MATS>
+__global__ void __launch_bounds__(128) k_postproc(ElemArgs<T> a, PostArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane8 = threadIdx.x & 7;
+  const int le = threadIdx.x >> 3;
+  const int epb = blockDim.x >> 3;
+  T* tab = reinterpret_cast<T*>(smem_raw);                       // [8][8][4]
+  double* rows_all = reinterpret_cast<double*>(tab + 256);       // [epb][8][PP_ROW]
+  T* nsm_all = reinterpret_cast<T*>(rows_all + epb * 8 * PP_ROW); // [epb][NODE_STRIDE]
+  MatC* msm = reinterpret_cast<MatC*>(nsm_all + epb * ElemSmem<T>::NODE_STRIDE) + le;
+  double* rows = rows_all + le * 8 * PP_ROW;
+  T* nsm = nsm_all + le * ElemSmem<T>::NODE_STRIDE;
+  const int64_t e = (int64_t)a.beg + (int64_t)blockIdx.x * epb + le;
+  const bool valid = e < a.end;
+  const int64_t ec = valid ? e : (int64_t)a.end - 1;
+  fill_hex8_table<T>(tab);
+
+  const int nid = a.lnods[8 * ec + lane8];
+  const double tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
+  if constexpr (MATS) {
+    const uint4* src = reinterpret_cast<const uint4*>(a.mats + __ldg(a.lmate + ec));
+    uint4* dst = reinterpret_cast<uint4*>(msm);
+    dst[lane8] = __ldg(src + lane8);
+    if (lane8 + 8 < MAT_CHUNKS) dst[8 + lane8] = __ldg(src + 8 + lane8);
+  }
+  double X[3], U[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    X[c] = __ldg(a.coord + c * a.npad + nid);
+    U[c] = __ldg(a.u + c * a.npad + nid);
+  }
+  const int src = (threadIdx.x & 31) & ~7;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    nsm[8 * c + lane8] = (T)(X[c] - __shfl_sync(0xffffffffu, X[c], src));
+    nsm[8 * (3 + c) + lane8] = (T)(U[c] - __shfl_sync(0xffffffffu, U[c], src));
+  }
+  const int64_t gp = 8 * ec + lane8;
+  double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp];
+  double F_SA = (double)a.sold[2 * a.sst + gp];
+  __syncthreads();                                               // table, node rows, materials
+
+  T Ji[9], H[9];
+  const T vol = gp_kinematics<T>(nsm, lane8, Ji, H);            // Gauss weight 1
+  T tau[6];
+  law160_tau<T>(elem_mat<MATS>(a, msm), H, tmp, xS, F_AS, F_SA, tau);
+  const T detF = (T(1) + H[0]) * ((T(1) + H[4]) * (T(1) + H[8]) - H[5] * H[7])
+               - H[1] * (H[3] * (T(1) + H[8]) - H[5] * H[6])
+               + H[2] * (H[3] * H[7] - (T(1) + H[4]) * H[6]);
+  const T iJ = Fm<T>::rcp(detF);
+  // Voigt (xx yy zz yz xz xy); tau and L come as (xx yy zz xy yz xz)
+  const double sig[6] = {(double)(tau[0] * iJ), (double)(tau[1] * iJ), (double)(tau[2] * iJ),
+                         (double)(tau[4] * iJ), (double)(tau[5] * iJ), (double)(tau[3] * iJ)};
+  T A[6], L[6], f[3];
+  A[0] = T(2) * H[0] + (H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
+  A[1] = T(2) * H[4] + (H[3] * H[3] + H[4] * H[4] + H[5] * H[5]);
+  A[2] = T(2) * H[8] + (H[6] * H[6] + H[7] * H[7] + H[8] * H[8]);
+  A[3] = H[1] + H[3] + (H[0] * H[3] + H[1] * H[4] + H[2] * H[5]);
+  A[4] = H[5] + H[7] + (H[3] * H[6] + H[4] * H[7] + H[5] * H[8]);
+  A[5] = H[2] + H[6] + (H[0] * H[6] + H[1] * H[7] + H[2] * H[8]);
+  sym_log1p(A, L, f);
+  // Green strain E_ij = (H_ij + H_ji + sum_k H_ki H_kj) / 2
+  auto gre = [&](int i, int j) -> double {
+    return 0.5 * ((double)H[3 * i + j] + (double)H[3 * j + i] + (double)H[i] * H[j] +
+                  (double)H[3 + i] * H[3 + j] + (double)H[6 + i] * H[6 + j]);
+  };
+  const double dv = (double)vol;
+  double* r = rows + lane8 * PP_ROW;
+#pragma unroll
+  for (int v = 0; v < 6; ++v) r[v] = dv * sig[v];
+  r[6] = dv * gre(0, 0);
+  r[7] = dv * gre(1, 1);
+  r[8] = dv * gre(2, 2);
+  r[9] = dv * gre(1, 2);
+  r[10] = dv * gre(0, 2);
+  r[11] = dv * gre(0, 1);
+  r[12] = dv * 0.5 * (double)L[0];
+  r[13] = dv * 0.5 * (double)L[1];
+  r[14] = dv * 0.5 * (double)L[2];
+  r[15] = dv * 0.5 * (double)L[4];
+  r[16] = dv * 0.5 * (double)L[5];
+  r[17] = dv * 0.5 * (double)L[3];
+  r[18] = dv;
+  if (p.gp_sig && valid) {
+    double* o = p.gp_sig + 6 * (8 * (int64_t)p.perm[ec] + lane8);
+#pragma unroll
+    for (int v = 0; v < 6; ++v) o[v] = sig[v];
+  }
+  __syncwarp();
+
+  // lane = node a: sum over the element's Gauss points
+  if (valid) {
+#pragma unroll 1
+    for (int k = 0; k < PP_COLS; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int g = 0; g < 8; ++g) s += (double)tab[32 * g + 4 * lane8 + 3] * rows[g * PP_ROW + k];
+      atomicAdd(p.acc + (int64_t)k * a.npad + nid, s);
+    }
+  }
+}
+
+// nodal values: X / vmass for the three tensors, von Mises of the Cauchy
+// stress (sld_calculate_pp_tensors.f90:98-142); out = [caust | green | lepsi]
+// each (6, npoin), then seqvm (npoin)
+__global__ void k_postproc_nodal(const double* acc, int64_t npad, int64_t npoin, double* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npoin) return;
+  const double inv = 1.0 / acc[(PP_COLS - 1) * npad + i];
+  double c[6];
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+      const double x = inv * acc[(6 * t + v) * npad + i];
+      out[t * 6 * npoin + 6 * i + v] = x;
+      if (t == 0) c[v] = x;
+    }
+  out[18 * npoin + i] = sqrt(0.5 * ((c[0] - c[1]) * (c[0] - c[1]) + (c[1] - c[2]) * (c[1] - c[2]) +
+                                    (c[2] - c[0]) * (c[2] - c[0]) +
+                                    6.0 * (c[3] * c[3] + c[4] * c[4] + c[5] * c[5])));
 }
 
 // ---------------------------------------------------------------------------

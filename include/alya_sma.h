@@ -136,6 +136,21 @@ int32_t sma_assemble_device(sma_ctx* ctx, const double* d_displ, double fext_sca
 /* sld_updunk(ITASK_ENDSTE) for the state: slot TIME_N <- slot ITER_K */
 int32_t sma_end_step(sma_ctx* ctx);
 
+/* Stress and strain post-processing, HOST buffers, any of them NULL:
+ * caust, green, lepsi (6,npoin): nodal Cauchy stress, Green-Lagrange strain
+ * and logarithmic strain in Voigt order xx yy zz yz xz xy, each the
+ * N_a dV-weighted average over the Gauss points around node a; seqvm (npoin)
+ * the von Mises stress of the nodal Cauchy stress; gp_sigma (6,8,nelem) the
+ * Cauchy stress per Gauss point.  The law is evaluated at the current
+ * displacement from the state the last element loop started from (TIME_N if
+ * none ran since the state was set), so after sma_explicit_step or
+ * sma_assemble it reproduces that loop's stresses; the state is not changed.
+ * Replaces sld_calculate_pp_tensors (sld_calculate_pp_tensors.f90:40-145)
+ * with sld_calculate_pp_tensors_ielem (sld_calculate_pp_tensors_ielem.f90:
+ * 100-150 and 180-218, itask 3 of sld_elmope). */
+int32_t sma_postprocess(sma_ctx* ctx, double* caust, double* green, double* lepsi,
+                        double* seqvm, double* gp_sigma);
+
 /* Material-plugin boundary, batched: n independent Gauss points with device
  * pointers F (9n), tmp (n or NULL), sdv_old/sdv_new (3n), pk2 (9n),
  * nr_flag (n or NULL).  Replaces eval_sld_stress_model_160 with flagt = 0

@@ -86,7 +86,11 @@ extern "C" {
                      int nthreads, T dtime, int nsteps, T* cutim, T* displ,         \
                      T* veloc, T* accel, T* sdv, T* rhsid, int nwit,                \
                      const int32_t* wit_dof, T* wit_hist, int32_t* counters,        \
-                     int scheme, T phi);
+                     int scheme, T phi);                                            \
+  int  orc_postprocess##S(int nelem, int npoin, const int32_t* lnods, const T* coord,\
+                          const T* displ, const int32_t* lmate, const T* props,     \
+                          const T* e_mart, const T* tempe, const T* sdv, int slot,  \
+                          T* caust, T* green, T* lepsi, T* seqvm, T* gp_sigma);
 
 ORC_DECL(double, _f64)
 ORC_DECL(float, _f32)

@@ -789,5 +789,132 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
   return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Stress and strain post-processing: sld_calculate_pp_tensors.f90:40-145    */
+/* with sld_calculate_pp_tensors_ielem.f90:100-150 (itask 3: Cauchy stress,  */
+/* Green strain) and :180-218 (logarithmic strain).  Per Gauss point          */
+/*   sigma(i,j) = sum_k F(i,k) P(j,k) / det F                                 */
+/*   E(i,j)     = sum_k F(k,i) F(k,j) / 2 - delta_ij / 2                      */
+/*   lnV(i,j)   = sum_k log(sqrt(|w_k|)) n_k(i) n_k(j),  (w, n) eig(F F^T)     */
+/* projected to the nodes as sum_e sum_g N_a(g) dV(g) X / vmass_a, vmass the  */
+/* volume-lumped mass of the kernel (mod_mass_matrix.f90:150-215, no          */
+/* density); von Mises of the nodal Cauchy stress (3-D branch, :135-142).     */
+/* The reference diagonalises b with maths_eigen_symmetric_matrix; the oracle */
+/* uses the Householder + QL solver above.  P comes from the law evaluated    */
+/* on the state slot `slot` of sdv (its new state is discarded), as the       */
+/* element loop that produced gppio.  Voigt order xx yy zz yz xz xy           */
+/* (nvgij_sld, sld_inivar.f90:568-579).  Outputs are (6, npoin) except seqvm  */
+/* (npoin) and gp_sigma (6, 8, nelem); any output may be NULL.                */
+/* ------------------------------------------------------------------------ */
+int FN(orc_postprocess)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
+                        const REAL* displ, const int32_t* lmate, const REAL* props,
+                        const REAL* e_mart, const REAL* tempe, const REAL* sdv, int slot,
+                        REAL* caust, REAL* green, REAL* lepsi, REAL* seqvm, REAL* gp_sigma)
+{
+  static const int vi[6] = {0, 1, 2, 1, 0, 0}, vj[6] = {0, 1, 2, 2, 2, 1};
+  REAL posgp[24], weigp[8];
+  FN(orc_hex8_gauss)(posgp, weigp);
+  REAL* acc = (REAL*)calloc(19 * (size_t)npoin, sizeof(REAL));   /* 6 + 6 + 6 + vmass */
+  if (!acc) return -1;
+  for (int e = 0; e < nelem; ++e) {
+    const int32_t* ln = lnods + 8 * (int64_t)e;
+    REAL elcod[24], eldis[24];
+    for (int a = 0; a < 8; ++a)
+      for (int i = 0; i < 3; ++i) {
+        elcod[i + 3 * a] = coord[i + 3 * (int64_t)ln[a]];
+        eldis[i + 3 * a] = displ[i + 3 * (int64_t)ln[a]];
+      }
+    const int im = lmate ? lmate[e] : 0;
+    const REAL em = e_mart ? e_mart[im] : (REAL)0;
+    const REAL tmp = tempe ? tempe[e] : (REAL)0;
+    for (int g = 0; g < 8; ++g) {
+      REAL shapf[8], deriv[24], xjaci[9], gpcar[24];
+      FN(orc_hex8_shape)(posgp[3 * g], posgp[3 * g + 1], posgp[3 * g + 2], shapf, deriv);
+      const REAL volux = weigp[g] * FN(jacobi3)(elcod, deriv, xjaci, gpcar);
+      REAL F[9];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          REAL s = 0;
+          for (int a = 0; a < 8; ++a) s = s + eldis[i + 3 * a] * gpcar[j + 3 * a];
+          M3(F, i, j) = s + (i == j ? (REAL)1 : (REAL)0);
+        }
+      REAL t1 = M3(F,1,1) * M3(F,2,2) - M3(F,2,1) * M3(F,1,2);
+      REAL t2 = -M3(F,1,0) * M3(F,2,2) + M3(F,2,0) * M3(F,1,2);
+      REAL t3 = M3(F,1,0) * M3(F,2,1) - M3(F,2,0) * M3(F,1,1);
+      const REAL detF = M3(F,0,0) * t1 + M3(F,0,1) * t2 + M3(F,0,2) * t3;
+      /* P as the element loop forms it (law 160, PK2 pull-back, PK1) */
+      REAL Finv[9], tau[9], S[9], P[9], st[3];
+      FN(inv3x3)(F, Finv);
+      for (int c = 0; c < 3; ++c) st[c] = sdv[48 * (int64_t)e + 24 * slot + 3 * g + c];
+      FN(orc_law160_kirchhoff)(props + 18 * im, em, F, tmp, st, tau);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          REAL s = 0;
+          for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) s = s + M3(Finv, i, k) * M3(Finv, j, l) * M3(tau, k, l);
+          M3(S, i, j) = s;
+        }
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+          REAL s = 0;
+          for (int i = 0; i < 3; ++i) s = s + M3(F, j, i) * M3(S, i, k);
+          M3(P, j, k) = s;
+        }
+      REAL sig[9], gre[9], b[9], Q[9], w[3], lep[9];
+      const REAL gpinv = (REAL)1 / detF;
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          REAL s = 0, r = 0, q = 0;
+          for (int k = 0; k < 3; ++k) {
+            s = s + gpinv * M3(F, i, k) * M3(P, j, k);
+            r = r + (REAL)0.5 * (M3(F, k, i) * M3(F, k, j));
+            q = q + M3(F, i, k) * M3(F, j, k);
+          }
+          M3(sig, i, j) = s;
+          M3(gre, i, j) = r - (i == j ? (REAL)0.5 : (REAL)0);
+          M3(b, i, j) = q;
+        }
+      int fail = 0;
+      FN(orc_dsyevq3)(b, Q, w, &fail);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          REAL s = 0;
+          for (int k = 0; k < 3; ++k) s = s + LOG(SQRT(FABS(w[k]))) * M3(Q, i, k) * M3(Q, j, k);
+          M3(lep, i, j) = s;
+        }
+      for (int a = 0; a < 8; ++a) {
+        REAL* ac = acc + 19 * (int64_t)ln[a];
+        const REAL xmean = shapf[a] * volux;
+        for (int v = 0; v < 6; ++v) {
+          ac[v] += xmean * M3(sig, vi[v], vj[v]);
+          ac[6 + v] += xmean * M3(gre, vi[v], vj[v]);
+          ac[12 + v] += xmean * M3(lep, vi[v], vj[v]);
+        }
+        ac[18] += xmean;
+      }
+      if (gp_sigma)
+        for (int v = 0; v < 6; ++v) gp_sigma[v + 6 * (g + 8 * (int64_t)e)] = M3(sig, vi[v], vj[v]);
+    }
+  }
+  for (int p = 0; p < npoin; ++p) {
+    const REAL* ac = acc + 19 * (int64_t)p;
+    const REAL dummr = (REAL)1 / ac[18];
+    for (int v = 0; v < 6; ++v) {
+      if (caust) caust[v + 6 * (int64_t)p] = dummr * ac[v];
+      if (green) green[v + 6 * (int64_t)p] = dummr * ac[6 + v];
+      if (lepsi) lepsi[v + 6 * (int64_t)p] = dummr * ac[12 + v];
+    }
+    if (seqvm) {
+      REAL c[6];
+      for (int v = 0; v < 6; ++v) c[v] = dummr * ac[v];
+      seqvm[p] = SQRT((REAL)0.5 * ((c[0] - c[1]) * (c[0] - c[1]) + (c[1] - c[2]) * (c[1] - c[2]) +
+                                   (c[2] - c[0]) * (c[2] - c[0]) +
+                                   (REAL)6 * (c[3] * c[3] + c[4] * c[4] + c[5] * c[5])));
+    }
+  }
+  free(acc);
+  return 0;
+}
+
 #undef FN
 #undef M3
