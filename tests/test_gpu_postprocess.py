@@ -80,7 +80,8 @@ def test_postprocess_per_element_materials_and_colour_order(oracle):
 
 def test_postprocess_after_steps_is_repeatable():
     """After a run of steps it reads the last loop's start state; calling it
-    twice gives the same result and leaves the run bit-for-bit unchanged."""
+    twice gives the same result (to the rounding of the FP64 atomic nodal
+    sums, whose order varies) and leaves the run bit-for-bit unchanged."""
     p = P.bar_40x4x4(nsteps=200)
     a = sma.ExplicitSolid(p, precision="fp64", scatter="color")
     b = sma.ExplicitSolid(p, precision="fp64", scatter="color")
@@ -89,7 +90,7 @@ def test_postprocess_after_steps_is_repeatable():
     r1 = a.postprocess()
     r2 = a.postprocess()
     for k in ("caust", "green", "lepsi", "seqvm"):
-        assert np.array_equal(r1[k], r2[k])
+        assert _rel(r2[k], r1[k]) < 1e-12, (k, _rel(r2[k], r1[k]))
     assert r1["seqvm"].max() > 0.0
     a.step(30)
     b.step(30)
