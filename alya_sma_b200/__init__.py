@@ -46,7 +46,7 @@ class _Mesh(C.Structure):
 
 class _Mat(C.Structure):
     _fields_ = [("nmate", C.c_int32), ("props", C.c_void_p), ("e_mart", C.c_void_p),
-                ("densi", C.c_void_p), ("tempe", C.c_void_p)]
+                ("densi", C.c_void_p), ("tempe", C.c_void_p), ("dampi", C.c_void_p)]
 
 
 class _Run(C.Structure):
@@ -153,11 +153,11 @@ class ExplicitSolid:
             tempe=_c(prob.tempe, np.float64), fixno=_c(prob.fixno, np.int32),
             bcfun=_c(prob.bcfun, np.int32), fun_npts=_c(prob.fun_npts, np.int32),
             fun_smooth=_c(prob.fun_smooth, np.int32), fun_tab=_c(prob.fun_tab, np.float64),
-            fext=_c(prob.fext, np.float64))
+            fext=_c(prob.fext, np.float64), dampi=_c(getattr(prob, "dampi", None), np.float64))
         k = self._keep
         mesh = _Mesh(self.nelem, self.npoin, _p(k["lnods"]), _p(k["coord"]), _p(k["lmate"]))
         mat = _Mat(k["props"].reshape(-1, 18).shape[0], _p(k["props"]), _p(k["e_mart"]),
-                   _p(k["densi"]), _p(k["tempe"]))
+                   _p(k["densi"]), _p(k["tempe"]), _p(k["dampi"]))
         run = _Run(PREC[precision], SCATTER[scatter], device, int(k["fun_npts"].size),
                    float(prob.dtime if dtime is None else dtime), _p(k["fixno"]), _p(k["bcfun"]),
                    _p(k["fun_npts"]), _p(k["fun_smooth"]), _p(k["fun_tab"]), _p(k["fext"]),

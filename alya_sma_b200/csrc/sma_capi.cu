@@ -247,12 +247,14 @@ struct sma_ctx {
   // scheme and energy balance
   int scheme = SMA_SCHEME_CD;
   bool energy = false;
+  bool damp = false;                       // some material has Rayleigh alpha > 0
   int ehist_max = 0;
   double* d_uprev = nullptr;
   double* d_fintp = nullptr;
   double* d_fextp = nullptr;
   double* d_en = nullptr;                  // [4..8] totals (ALLIE, ALLWK, ALLKE, EENER, steps)
   double* d_epart = nullptr;               // per-block partial sums of the nodal kernel
+  double* d_fray = nullptr;                // Rayleigh alpha nodal force (damped runs), SoA
   double* d_ehist = nullptr;
   int* d_erow = nullptr;
   // host copies
@@ -276,9 +278,19 @@ struct sma_ctx {
 
 namespace {
 
+// Rayleigh alpha velocity: what the reference's element loop gathers from
+// veloc(ITER_K) -- inside a step the boundary velocity v_n (central
+// difference) or the predicted v_n + dt a_n (Tchamwa-Wielgosz); outside a
+// step (sma_assemble) the velocity field as set
+const double* damp_velocity(const sma_ctx* c, bool stepping) {
+  if (!c->damp) return nullptr;
+  return (stepping && c->scheme == SMA_SCHEME_TW) ? c->d_vt : c->d_v;
+}
+
 template <typename T>
-ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance) {
+ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance, bool stepping = false) {
   ElemArgs<T> a;
+  a.vel = damp_velocity(c, stepping);
   a.lnods = c->d_lnods;
   a.coord = c->d_coord;
   a.u = c->d_u;
@@ -319,6 +331,10 @@ ElemKernel<T> elem_kernel(const sma_ctx* c) {
   const bool pipe = c->variant == SMA_VARIANT_PIPE;
   const bool atomic = c->scatter != SMA_SCATTER_COLOR;
   const bool mats = c->d_lmate != nullptr;
+  if (c->damp) {                                                 // one-tile kernel only
+    if (atomic) return mats ? k_element<T, true, true, true> : k_element<T, true, false, true>;
+    return mats ? k_element<T, false, true, true> : k_element<T, false, false, true>;
+  }
   if (atomic) return mats ? elem_kernel_v<T, true, true>(pipe) : elem_kernel_v<T, true, false>(pipe);
   return mats ? elem_kernel_v<T, false, true>(pipe) : elem_kernel_v<T, false, false>(pipe);
 }
@@ -359,7 +375,7 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
   for (int r = 0; r < nrange; ++r) {
     const int beg = c->cptr[r], end = c->cptr[r + 1];
     if (end <= beg) continue;
-    ElemArgs<T> a = elem_args<T>(c, beg, end, advance && r == 0);
+    ElemArgs<T> a = elem_args<T>(c, beg, end, advance && r == 0, advance);
     const int64_t ntiles = ceil_div(end - beg, epb);
     const unsigned grid = c->variant == SMA_VARIANT_PIPE
                               ? (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident)
@@ -414,9 +430,21 @@ NodalArgs nodal_args(sma_ctx* c) {
   a.fint_prev = c->d_fintp;
   a.fext_prev = c->d_fextp;
   a.en_step = c->d_epart;
+  a.fray = (c->damp && c->energy) ? c->d_fray : nullptr;
+  a.store_v = (c->damp && c->scheme == SMA_SCHEME_CD) ? 1 : 0;
   a.npoin = c->npoin;
   a.npad = c->npad;
   return a;
+}
+
+// the Rayleigh alpha force alone into d_fray (energy balance, finte)
+int32_t launch_rayleigh(sma_ctx* c, const double* vel) {
+  CU(cudaMemsetAsync(c->d_fray, 0, 3 * (size_t)c->npad * sizeof(double), c->stream));
+  k_rayleigh<<<(unsigned)ceil_div(c->nelem, 128), 128, 0, c->stream>>>(
+      c->d_lnods, c->d_coord, vel, c->d_lmate, c->d_mats, c->mat0, c->nelem, c->npad, c->d_fray);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
 }
 
 template <int MODE>
@@ -465,6 +493,7 @@ int32_t issue_step(sma_ctx* c, int nodal_mode) {
   c->cur ^= 1;   // the state written by this step is TIME_N of the next
   // u holds u_k until the nodal kernel predicts u_{k+1}
   if ((rc = launch_witness(c))) return rc;
+  if (c->damp && c->energy && (rc = launch_rayleigh(c, damp_velocity(c, true)))) return rc;
   return launch_nodal(c, nodal_mode);
 }
 
@@ -488,6 +517,7 @@ int32_t issue_step_timed(sma_ctx* c, int nodal_mode) {
   c->cur ^= 1;
   if ((rc = next_event(c, &e1))) return rc;
   if ((rc = launch_witness(c))) return rc;
+  if (c->damp && c->energy && (rc = launch_rayleigh(c, damp_velocity(c, true)))) return rc;
   if ((rc = launch_nodal(c, nodal_mode))) return rc;
   if ((rc = next_event(c, &e2))) return rc;
   c->evmarks.push_back({0, {e0, e1}});
@@ -543,7 +573,8 @@ int32_t build_graphs(sma_ctx* c, int chunk) {
 }
 
 int64_t kernels_per_step(const sma_ctx* c) {
-  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0);
+  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0) +
+         (c->energy && c->damp ? 1 : 0);
 }
 
 template <typename T>
@@ -574,7 +605,7 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
                   c->d_fextp, c->d_en, c->d_ehist, c->d_erow, c->d_epart, c->d_pp_acc,
-                  c->d_pp_out, c->d_pp_gp};
+                  c->d_pp_out, c->d_pp_gp, c->d_fray};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -597,6 +628,14 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
     return fail(SMA_ERR_ARG, "block must be a multiple of 32 in [32, 256]");
   if (run->scheme != SMA_SCHEME_CD && run->scheme != SMA_SCHEME_TW)
     return fail(SMA_ERR_ARG, "scheme must be SMA_SCHEME_CD or SMA_SCHEME_TW");
+  if (mat->dampi)
+    for (int im = 0; im < mat->nmate; ++im) {
+      if (!(mat->dampi[2 * im] >= 0.0))
+        return fail(SMA_ERR_ARG, "Rayleigh alpha of material " + std::to_string(im) + " must be >= 0");
+      if (mat->dampi[2 * im + 1] != 0.0)
+        return fail(SMA_ERR_ARG, "Rayleigh beta (stiffness-proportional damping) of material " +
+                                     std::to_string(im) + " is not supported; use alpha only");
+    }
   for (int64_t k = 0; k < 8 * (int64_t)mesh->nelem; ++k)
     if (mesh->lnods[k] < 0 || mesh->lnods[k] >= mesh->npoin)
       return fail(SMA_ERR_ARG, "lnods entry out of range at " + std::to_string(k));
@@ -697,8 +736,12 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
     TRYCU(cudaMemcpy(c->d_tempe, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   std::vector<MatC> mats(c->nmate);
-  for (int im = 0; im < c->nmate; ++im)
+  for (int im = 0; im < c->nmate; ++im) {
     mats[im] = make_mat(mat->props + 18 * im, mat->e_mart ? mat->e_mart[im] : 0.0, mat->densi[im]);
+    mats[im].ray_a = mat->dampi ? mat->dampi[2 * im] : 0.0;
+    c->damp |= mats[im].ray_a > 0.0;
+  }
+  if (c->damp) c->variant = SMA_VARIANT_PLAIN;                  // the damped kernel is one-tile
   TRY(dalloc(&c->d_mats, mats.size() * sizeof(MatC)));
   TRYCU(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(MatC), cudaMemcpyHostToDevice));
   c->mat0 = mats[0];
@@ -709,6 +752,10 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   for (double** p : nodal) {
     TRY(dalloc(p, nb));
     TRYCU(cudaMemset(*p, 0, nb));
+  }
+  if (c->damp) {
+    TRY(dalloc(&c->d_fray, nb));
+    TRYCU(cudaMemset(c->d_fray, 0, nb));
   }
   TRY(dalloc(&c->d_stage, 3 * (size_t)c->npoin * sizeof(double)));
   TRY(dalloc(&c->d_stage2, 3 * (size_t)c->npoin * sizeof(double)));
@@ -834,7 +881,7 @@ int32_t sma_assemble_device(sma_ctx* c, const double* d_displ, double fext_scale
   int32_t rc = launch_elements(c, false);
   if (rc) return rc;
   k_outputs<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin,
-                                          c->npad, d_rhsid, nullptr, nullptr, nullptr);
+                                          c->npad, d_rhsid, nullptr, nullptr, nullptr, nullptr);
   c->launches++;
   CU(cudaGetLastError());
   return SMA_OK;
@@ -854,13 +901,19 @@ int32_t sma_assemble(sma_ctx* c, const double* displ, double fext_scale, double*
   int32_t rc = launch_elements(c, false);
   if (rc) return rc;
   double* outs[4] = {rhsid, finte, fexte, frxid};
+  // with damping, finte leaves the Rayleigh force out (it is in rhsid only)
+  const double* fray = nullptr;
+  if (c->damp && finte) {
+    if ((rc = launch_rayleigh(c, damp_velocity(c, false)))) return rc;
+    fray = c->d_fray;
+  }
   for (int q = 0; q < 4; ++q) {
     if (!outs[q]) continue;
     double* dr = c->d_stage;
     k_outputs<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin,
                                             c->npad, q == 0 ? dr : c->d_stage2,
                                             q == 1 ? dr : nullptr, q == 2 ? dr : nullptr,
-                                            q == 3 ? dr : nullptr);
+                                            q == 3 ? dr : nullptr, fray);
     c->launches++;
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(outs[q], dr, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -1339,6 +1392,7 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   a.beg = 0;
   a.end = nelem;
   a.has_grav = 0;
+  a.vel = nullptr;
   const int block = 256, epb = block / 8;
   const size_t smem = element_smem_bytes<T>(block, false);      // below the 48 KB default
   k_element<T, true, false><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);

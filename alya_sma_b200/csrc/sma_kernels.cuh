@@ -114,6 +114,7 @@ struct ElemArgs {
   int32_t beg, end;            // element range of this launch
   double grav[3];              // rho-scaled body force per unit mass (elfext)
   int has_grav;
+  const double* vel;           // SoA [3][npad] velocity for Rayleigh alpha, or null
   MatC mat0;                   // the material when lmate is null (kernel-parameter space)
 };
 
@@ -222,15 +223,17 @@ __device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H) {
 // element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
 // Gauss point a, `mat` the element's material (the kernel parameter for a
 // one-material mesh, so its constants are instruction operands; a shared-
-// memory copy otherwise) and `tmp` its temperature.  Stages the node rows,
-// then phase 1 (lane = Gauss point), the law, phase 2 (lane = node) and the
-// scatter-add.  Needs the block's reference table in `tab`.
-template <typename T, bool ATOMIC>
+// memory copy otherwise), `tmp` its temperature and Vn node a's velocity
+// (read only in the DAMP instance, which adds the Rayleigh alpha force; the
+// others keep the register budget of the undamped step).  Stages the node
+// rows, then phase 1 (lane = Gauss point), the law, phase 2 (lane = node) and
+// the scatter-add.  Needs the block's reference table in `tab`.
+template <typename T, bool ATOMIC, bool DAMP = false>
 __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab, T* nsm, T* qsm,
                                              int lane8, bool valid, int64_t ec, int nid,
                                              const double* dX, const double* dU,
                                              double xS, double F_AS, double F_SA,
-                                             const MatC& mat, double tmp) {
+                                             const MatC& mat, double tmp, const T* Vn) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     nsm[8 * c + lane8] = (T)dX[c];
@@ -274,12 +277,37 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
     q[3 + m] = t01 * B[3 * m + 0] + t11 * B[3 * m + 1] + t12 * B[3 * m + 2];
     q[6 + m] = t02 * B[3 * m + 0] + t12 * B[3 * m + 1] + t22 * B[3 * m + 2];
   }
-  q[9] = vol * (T)mat.densi;
+  // body force of the Gauss point, dV rho (g - alpha v(g)): gravity
+  // (elfext) and the Rayleigh alpha term (elrayl_alpha, sld_elmmat.f90:156-
+  // 159) with v(g) = sum_b N_b(g) v_b from the element's lanes by shuffle
+  const bool body = DAMP || a.has_grav;
+  if (body) {
+    const T rho = (T)mat.densi;
+    T b0 = rho * (T)a.grav[0], b1 = rho * (T)a.grav[1], b2 = rho * (T)a.grav[2];
+    if constexpr (DAMP) {
+      T N[8], dN[24];
+      hex8_gp<T>(lane8, N, dN);
+      const int src = (threadIdx.x & 31) & ~7;
+      T v0 = T(0), v1 = T(0), v2 = T(0);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        v0 += N[b] * __shfl_sync(0xffffffffu, Vn[0], src + b);
+        v1 += N[b] * __shfl_sync(0xffffffffu, Vn[1], src + b);
+        v2 += N[b] * __shfl_sync(0xffffffffu, Vn[2], src + b);
+      }
+      const T ra = rho * (T)mat.ray_a;
+      b0 -= ra * v0;
+      b1 -= ra * v1;
+      b2 -= ra * v2;
+    }
+    q[9] = vol * b0;
+    q[10] = vol * b1;
+    q[11] = vol * b2;
+  }
   __syncwarp();
 
   // ---- phase 2, lane = node a: sum the 8 Gauss points ---------------------
   T f0 = T(0), f1 = T(0), f2 = T(0);
-  const T gx = (T)a.grav[0], gy = (T)a.grav[1], gz = (T)a.grav[2];
 #pragma unroll
   for (int g = 0; g < 8; ++g) {
     T qg[12], dn[4];
@@ -290,11 +318,10 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
     f0 -= qg[0] * dn[0] + qg[1] * dn[1] + qg[2] * dn[2];
     f1 -= qg[3] * dn[0] + qg[4] * dn[1] + qg[5] * dn[2];
     f2 -= qg[6] * dn[0] + qg[7] * dn[1] + qg[8] * dn[2];
-    if (a.has_grav) {
-      const T w = dn[3] * qg[9];
-      f0 += w * gx;
-      f1 += w * gy;
-      f2 += w * gz;
+    if (body) {
+      f0 += dn[3] * qg[9];
+      f1 += dn[3] * qg[10];
+      f2 += dn[3] * qg[11];
     }
   }
   if (valid) {
@@ -339,8 +366,8 @@ constexpr int elem_min_blocks() { return (sizeof(T) == 4 && !PIPE && !MATS) ? 3 
 // One tile of elements per block: each lane gathers its node with __ldg,
 // takes node 1's values from lane 0 of its element by shuffle.  MATS: the
 // mesh has per-element materials (lmate), copied into shared memory per
-// element.
-template <typename T, bool ATOMIC, bool MATS>
+// element.  DAMP: Rayleigh alpha damping with the velocity a.vel.
+template <typename T, bool ATOMIC, bool MATS, bool DAMP = false>
 __global__ void __launch_bounds__(256, (elem_min_blocks<T, false, MATS>())) k_element(ElemArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tab = reinterpret_cast<T*>(smem_raw);                       // [8][8][4]
@@ -381,9 +408,14 @@ __global__ void __launch_bounds__(256, (elem_min_blocks<T, false, MATS>())) k_el
   const int64_t gp = 8 * ec + lane8;
   const double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp];
   const double F_SA = (double)a.sold[2 * a.sst + gp];
+  T Vn[3] = {T(0), T(0), T(0)};
+  if constexpr (DAMP) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Vn[c] = (T)__ldg(a.vel + c * a.npad + nid);
+  }
   __syncthreads();                                               // reference table, materials
-  element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA,
-                          elem_mat<MATS>(a, msm), tmp);
+  element_tile<T, ATOMIC, DAMP>(a, tab, nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA,
+                                elem_mat<MATS>(a, msm), tmp, Vn);
 }
 
 // ---------------------------------------------------------------------------
@@ -496,9 +528,10 @@ __global__ void __launch_bounds__(256, (elem_min_blocks<T, true, MATS>())) k_ele
       dU[c] = nd[6 * lane8 + 3 + c] - nd[3 + c];
     }
     const double tmp = a.tempe ? *reinterpret_cast<const double*>(st + PS::TEMP_OFF) : 0.0;
+    const T Vn[3] = {T(0), T(0), T(0)};                         // undamped runs only
     element_tile<T, ATOMIC>(a, tab, nsm, qsm, lane8, v0, ec0, nid0, dX, dU, (double)ss[0],
                             (double)ss[1], (double)ss[2],
-                            elem_mat<MATS>(a, reinterpret_cast<const MatC*>(st + PS::MAT_OFF)), tmp);
+                            elem_mat<MATS>(a, reinterpret_cast<const MatC*>(st + PS::MAT_OFF)), tmp, Vn);
     __syncwarp();                                                // stage s is reused next-but-one
     nid0 = nid1; ec0 = ec1; v0 = v1;
     nid1 = nid2; ec1 = ec2; v1 = v2; im1 = im2;
@@ -696,6 +729,8 @@ struct NodalArgs {
   double* fint_prev;
   double* fext_prev;
   double* en_step;
+  const double* fray;     // Rayleigh alpha nodal force of the step (kept out of fint), or null
+  int store_v;            // MODE 1 also stores the step-boundary velocity (damped CD runs)
   int64_t npoin, npad;
 };
 
@@ -739,7 +774,8 @@ __global__ void __launch_bounds__(256) k_nodal(NodalArgs a) {
         if (ENERGY) {                                     // mod_sld_energy.f90:71-193
           const double uk = a.u[k];
           const double fx = (fl & 8u) ? a.fext[k] * ts.load : 0.0;
-          const double fi = fx - r;
+          // r = fext - fint - f_rayleigh (sld_elmmat.f90:168)
+          const double fi = fx - r - (a.fray ? a.fray[k] : 0.0);
           const double dd = uk - a.uprev[k];
           e_ie += (fi + a.fint_prev[k]) * dd;
           e_wk += (fx + a.fext_prev[k]) * dd;
@@ -754,6 +790,7 @@ __global__ void __launch_bounds__(256) k_nodal(NodalArgs a) {
         a.acc[k] = aa;
         a.v[k] = vv;
       } else {
+        if (MODE == 1 && a.store_v) a.v[k] = vv;                  // v_n for the next damping term
         double vn, un;
         if (SCHEME == SCHEME_CD) {
           vn = vv + ts.nx_c_pred * aa;                    // v at the half step k+1/2
@@ -881,7 +918,7 @@ __global__ void k_fill_f(double* f, const double* fext, const uint8_t* flags, do
 // loads), frxid = element part of rhsid on prescribed dofs
 __global__ void k_outputs(const double* f, const double* fext, const uint8_t* flags,
                           double scale, int64_t npoin, int64_t npad, double* rhsid,
-                          double* finte, double* fexte, double* frxid) {
+                          double* finte, double* fexte, double* frxid, const double* fray) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoin) return;
   const uint8_t fl = flags[p];
@@ -891,9 +928,58 @@ __global__ void k_outputs(const double* f, const double* fext, const uint8_t* fl
     const double fx = (fext && (fl & 8u)) ? fext[k] * scale : 0.0;
     rhsid[3 * p + c] = r;
     if (fexte) fexte[3 * p + c] = fx;
-    if (finte) finte[3 * p + c] = fx - r;
+    if (finte) finte[3 * p + c] = fx - r - (fray ? fray[k] : 0.0);   // damping kept out
     if (frxid) frxid[3 * p + c] = (fl & (1u << c)) ? r - fx : 0.0;
   }
+}
+
+// The Rayleigh alpha nodal force alone, sum_e sum_g N_a(g) dV rho alpha v(g)
+// (elrayl_alpha of sld_elmmat.f90:156-159), FP64, one thread per element,
+// added into fray (SoA [3][npad], zeroed by the caller).  The element kernel
+// already folds this force into the residual; this pass exists so that the
+// internal force of the energy balance and of sma_assemble's finte leaves it
+// out, as the reference does.
+__global__ void k_rayleigh(const int32_t* lnods, const double* coord, const double* vel,
+                           const int32_t* lmate, const MatC* mats, MatC mat0, int64_t nelem,
+                           int64_t npad, double* fray) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nelem) return;
+  const MatC& m = lmate ? mats[lmate[e]] : mat0;
+  if (!(m.ray_a > 0.0)) return;
+  int nd[8];
+  double X[8][3], V[8][3];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    nd[b] = lnods[8 * e + b];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      X[b][c] = coord[c * npad + nd[b]];
+      V[b][c] = vel[c * npad + nd[b]];
+    }
+  }
+  double f[8][3];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) f[b][0] = f[b][1] = f[b][2] = 0.0;
+  const double ra = m.ray_a * m.densi;
+  for (int g = 0; g < 8; ++g) {
+    double N[8], dN[24];
+    hex8_gp<double>(g, N, dN);
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0};
+    for (int b = 0; b < 8; ++b)
+      for (int c = 0; c < 3; ++c) {
+        J[3 * c + 0] += X[b][c] * dN[3 * b + 0];
+        J[3 * c + 1] += X[b][c] * dN[3 * b + 1];
+        J[3 * c + 2] += X[b][c] * dN[3 * b + 2];
+        v[c] += N[b] * V[b][c];
+      }
+    const double detJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                        J[2] * (J[3] * J[7] - J[4] * J[6]);
+    const double w = ra * detJ;                                  // Gauss weight 1
+    for (int b = 0; b < 8; ++b)
+      for (int c = 0; c < 3; ++c) f[b][c] += w * N[b] * v[c];
+  }
+  for (int b = 0; b < 8; ++b)
+    for (int c = 0; c < 3; ++c) atomicAdd(fray + c * npad + nd[b], f[b][c]);
 }
 
 // state layout: reference (3, 8, 2, nelem) <-> SoA [3][sst] per slot

@@ -46,6 +46,8 @@ struct MatC {
   double densi;
   int ext_E;                    // 1: E depends on xS0
   int pad;
+  double ray_a;                 // Rayleigh alpha (mass-proportional damping), 0: none
+  double pad2;
 };
 
 // ---------------------------------------------------------------------------

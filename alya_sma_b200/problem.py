@@ -78,6 +78,7 @@ class Problem:
     lmate: np.ndarray | None = None   # (nelem,) int32 material id
     tempe: np.ndarray | None = None   # (nelem,) temperature (extension)
     fext: np.ndarray | None = None    # (npoin, 3) nodal load at load factor 1
+    dampi: np.ndarray | None = None   # (nmate, 2) Rayleigh (alpha, beta) per material
     load_fun: int = -1                # table scaling fext (column v_x)
     dtime: float = 0.0                # time step (0: not chosen yet)
     nsteps: int = 0

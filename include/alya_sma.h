@@ -79,6 +79,10 @@ typedef struct {
   const double* e_mart;     /* (nmate) martensite modulus (extension) or NULL  */
   const double* densi;      /* (nmate) density after mass scaling              */
   const double* tempe;      /* (nelem) temperature (extension) or NULL         */
+  const double* dampi;      /* (2, nmate) Rayleigh (alpha, beta) or NULL:       */
+                            /* RAYLEIGH_DAMPING of sld_reaphy.f90:1048-1055;    */
+                            /* alpha (mass-proportional, sld_elmmat.f90:156-159) */
+                            /* is applied; beta > 0 is rejected (SMA_ERR_ARG)   */
 } sma_material_desc;
 
 typedef struct {

@@ -161,6 +161,8 @@ class Problem:
         self.fun_tab = np.ascontiguousarray(p.fun_tab, dtype=npt)
         self.fext = None if p.fext is None else np.ascontiguousarray(p.fext, dtype=npt)
         self.load_fun = int(p.load_fun)
+        dampi = getattr(p, "dampi", None)
+        self.dampi = None if dampi is None else np.ascontiguousarray(dampi, dtype=npt).reshape(-1, 2)
         nc, cp, ce, _ = color_elements(self.lnods, self.npoin)
         self.ncolor, self.color_ptr, self.color_elem = nc, cp, ce
         self.reset()
@@ -175,12 +177,14 @@ class Problem:
         self.rhsid = np.zeros((self.npoin, 3), npt)
         self.counters = np.zeros(NCOUNTERS, np.int32)
 
-    def assemble(self, displ=None, want_all=False, fext_scale=0.0):
-        """One element loop (sld_matrix explicit) at the given displacement.
+    def assemble(self, displ=None, want_all=False, fext_scale=0.0, veloc=None):
+        """One element loop (sld_matrix explicit) at the given displacement
+        (and, with Rayleigh damping, nodal velocity).
 
         Reads state slot TIME_N, writes slot ITER_K.  Returns a dict."""
         ct = self.ct
         d = self.displ if displ is None else np.ascontiguousarray(displ, dtype=self.dtype)
+        v = None if veloc is None else np.ascontiguousarray(veloc, dtype=self.dtype)
         n3 = (self.npoin, 3)
         out = {k: np.zeros(n3, self.dtype) for k in ("rhsid", "finte", "fexte", "frxid")}
         out["vmass"] = np.zeros(self.npoin, self.dtype)
@@ -193,7 +197,7 @@ class Problem:
            _ptr(self.color_ptr, C.c_int32), _ptr(self.color_elem, C.c_int32), self.nthreads,
            _ptr(out["rhsid"], ct), _ptr(out["finte"], ct), _ptr(out["fexte"], ct),
            _ptr(out["frxid"], ct), _ptr(out["vmass"], ct), _ptr(dmin, ct),
-           _ptr(self.counters, C.c_int32))
+           _ptr(self.counters, C.c_int32), _ptr(v, ct), _ptr(self.dampi, ct))
         out["gpdet_min"] = float(dmin[0])
         return out
 
@@ -247,5 +251,6 @@ class Problem:
            _ptr(self.color_elem, C.c_int32), self.nthreads, ct(dtime), int(nsteps),
            _ptr(self.cutim, ct), _ptr(self.displ, ct), _ptr(self.veloc, ct), _ptr(self.accel, ct),
            _ptr(self.sdv, ct), _ptr(self.rhsid, ct), int(wit.size), _ptr(wit, C.c_int32),
-           _ptr(hist, ct), _ptr(self.counters, C.c_int32), 1 if scheme == "tw" else 0, ct(phi))
+           _ptr(hist, ct), _ptr(self.counters, C.c_int32), 1 if scheme == "tw" else 0, ct(phi),
+           _ptr(self.dampi, ct))
         return hist[:, : wit.size]

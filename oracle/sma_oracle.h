@@ -64,7 +64,8 @@ extern "C" {
   int  orc_element##S(const T elcod[24], const T eldis[24], const T props[18],      \
                       T e_mart, T densi, T tmp, const T gravi[3],                   \
                       const T* sdv_old, T* sdv_new, T elfint[24], T elfext[24],     \
-                      T elmuu[8], T gppio[72], T* gpdet_min, int* nr_counts);       \
+                      T elmuu[8], T gppio[72], T* gpdet_min, int* nr_counts,        \
+                      const T* elvel, T ray_alpha, T elrayl[24]);                   \
   int  orc_assemble##S(int nelem, int npoin, const int32_t* lnods, const T* coord,  \
                        const T* displ, const int32_t* lmate, const T* props,        \
                        const T* e_mart, const T* densi, const T* tempe,             \
@@ -72,7 +73,8 @@ extern "C" {
                        const int32_t* fixno, T* sdv, int ncolor,                    \
                        const int32_t* color_ptr, const int32_t* color_elem,         \
                        int nthreads, T* rhsid, T* finte, T* fexte, T* frxid,        \
-                       T* vmass, T* gpdet_min, int32_t* counters);                  \
+                       T* vmass, T* gpdet_min, int32_t* counters,                   \
+                       const T* veloc, const T* dampi);                             \
   T    orc_funbou##S(int npts, const T* tab, int smooth, int idime, T cutim);       \
   T    orc_critical_dt##S(int nelem, const int32_t* lnods, const T* coord,          \
                           const int32_t* lmate, const T* props, const T* densi);    \
@@ -86,7 +88,7 @@ extern "C" {
                      int nthreads, T dtime, int nsteps, T* cutim, T* displ,         \
                      T* veloc, T* accel, T* sdv, T* rhsid, int nwit,                \
                      const int32_t* wit_dof, T* wit_hist, int32_t* counters,        \
-                     int scheme, T phi);                                            \
+                     int scheme, T phi, const T* dampi);                            \
   int  orc_postprocess##S(int nelem, int npoin, const int32_t* lnods, const T* coord,\
                           const T* displ, const int32_t* lmate, const T* props,     \
                           const T* e_mart, const T* tempe, const T* sdv, int slot,  \

@@ -489,11 +489,14 @@ REAL FN(orc_hex8_celen)(const REAL elcod[24])
 int FN(orc_element)(const REAL elcod[24], const REAL eldis[24], const REAL props[18],
                     REAL e_mart, REAL densi, REAL tmp, const REAL gravi[3],
                     const REAL* sdv_old, REAL* sdv_new, REAL elfint[24], REAL elfext[24],
-                    REAL elmuu[8], REAL gppio[72], REAL* gpdet_min, int* nr_counts)
+                    REAL elmuu[8], REAL gppio[72], REAL* gpdet_min, int* nr_counts,
+                    const REAL* elvel, REAL ray_alpha, REAL elrayl[24])
 {
   REAL posgp[24], weigp[8];
   FN(orc_hex8_gauss)(posgp, weigp);
   for (int i = 0; i < 24; ++i) { elfint[i] = 0; elfext[i] = 0; }
+  if (elrayl)
+    for (int i = 0; i < 24; ++i) elrayl[i] = 0;
   for (int a = 0; a < 8; ++a) elmuu[a] = 0;
 
   for (int g = 0; g < 8; ++g) {
@@ -548,14 +551,21 @@ int FN(orc_element)(const REAL elcod[24], const REAL eldis[24], const REAL props
         M3(P, j, k) = s;
       }
 
-    /* internal/external forces, sld_elmmat.f90:137-166 (no prestress,
-     * no Rayleigh damping) */
+    /* internal/external forces, sld_elmmat.f90:137-166 (no prestress), and
+     * the Rayleigh alpha force alpha v(g) N_a rho dV with the Gauss-point
+     * velocity v(g) = sum_b N_b elvel_b (sld_elmpre.f90:114, :160-163) */
+    REAL gpvel[3] = {0, 0, 0};
+    if (elvel && ray_alpha > 0)
+      for (int i = 0; i < 3; ++i)
+        for (int b = 0; b < 8; ++b) gpvel[i] = gpvel[i] + elvel[i + 3 * b] * shapf[b];
     for (int a = 0; a < 8; ++a)
       for (int i = 0; i < 3; ++i) {
         REAL s = elfint[i + 3 * a];
         for (int j = 0; j < 3; ++j) s = s + M3(P, i, j) * gpcar[j + 3 * a] * volux;
         elfint[i + 3 * a] = s;
         elfext[i + 3 * a] = elfext[i + 3 * a] + (shapf[a] * densi * volux) * gravi[i];
+        if (elrayl && elvel && ray_alpha > 0)
+          elrayl[i + 3 * a] = elrayl[i + 3 * a] + ray_alpha * gpvel[i] * shapf[a] * densi * volux;
       }
     /* lumped mass, sld_elmmat.f90:199-209 */
     for (int a = 0; a < 8; ++a)
@@ -569,7 +579,12 @@ int FN(orc_element)(const REAL elcod[24], const REAL eldis[24], const REAL props
  * loop (sld_elmope.f90:53-99), scatter-add (mod_matrix.f90:2327-2431 via
  * sld_element_operations.f90:239-256), Neumann nodal loads.  State is read
  * from slot TIME_N and written to slot ITER_K of sdv.  Any output pointer
- * may be NULL except rhsid and vmass. */
+ * may be NULL except rhsid and vmass.  dampi (2, nmate) holds the Rayleigh
+ * coefficients (alpha, beta) of sld_reaphy.f90:1048-1055 (NULL: none); the
+ * alpha force uses the nodal velocity veloc (the ITER_K velocity the element
+ * loop gathers, sld_elmgat.f90:60) and enters rhsid and frxid only, not
+ * finte or fexte (sld_elmmat.f90:168).  beta is not restated (see
+ * orc_run_cd). */
 int FN(orc_assemble)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
                      const REAL* displ, const int32_t* lmate, const REAL* props,
                      const REAL* e_mart, const REAL* densi, const REAL* tempe,
@@ -577,7 +592,8 @@ int FN(orc_assemble)(int nelem, int npoin, const int32_t* lnods, const REAL* coo
                      const int32_t* fixno, REAL* sdv, int ncolor,
                      const int32_t* color_ptr, const int32_t* color_elem,
                      int nthreads, REAL* rhsid, REAL* finte, REAL* fexte, REAL* frxid,
-                     REAL* vmass, REAL* gpdet_min, int32_t* counters)
+                     REAL* vmass, REAL* gpdet_min, int32_t* counters,
+                     const REAL* veloc, const REAL* dampi)
 {
   const REAL zero3[3] = {0, 0, 0};
   const REAL* grav = gravi ? gravi : zero3;
@@ -602,22 +618,27 @@ int FN(orc_assemble)(int nelem, int npoin, const int32_t* lnods, const REAL* coo
       for (int kk = beg; kk < end; ++kk) {
         int e = color_elem[kk];
         const int32_t* ln = lnods + 8 * (int64_t)e;
-        REAL elcod[24], eldis[24], elfint[24], elfext[24], elmuu[8], gppio[72];
+        REAL elcod[24], eldis[24], elvel[24], elfint[24], elfext[24], elmuu[8], gppio[72];
+        REAL elrayl[24];
         for (int a = 0; a < 8; ++a)
           for (int i = 0; i < 3; ++i) {     /* sld_elmgat.f90:53-63 */
             elcod[i + 3 * a] = coord[i + 3 * (int64_t)ln[a]];
             eldis[i + 3 * a] = displ[i + 3 * (int64_t)ln[a]];
+            elvel[i + 3 * a] = veloc ? veloc[i + 3 * (int64_t)ln[a]] : (REAL)0;
           }
         int im = lmate ? lmate[e] : 0;
         REAL em = e_mart ? e_mart[im] : (REAL)0;
         REAL tmp = tempe ? tempe[e] : (REAL)0;
+        REAL alpha = dampi ? dampi[2 * im] : (REAL)0;
         REAL* sd = sdv + 48 * (int64_t)e;
         FN(orc_element)(elcod, eldis, props + 18 * im, em, densi[im], tmp, grav,
-                        sd + 24, sd, elfint, elfext, elmuu, gppio, &ldmin, lcnt);
+                        sd + 24, sd, elfint, elfext, elmuu, gppio, &ldmin, lcnt,
+                        veloc ? elvel : NULL, alpha, elrayl);
         for (int a = 0; a < 8; ++a) {
           int64_t p = ln[a];
           for (int i = 0; i < 3; ++i) {
-            REAL elrhs = elfext[i + 3 * a] - elfint[i + 3 * a];
+            /* elrhs = elfext - elfint - elrayl_alpha, sld_elmmat.f90:168 */
+            REAL elrhs = elfext[i + 3 * a] - elfint[i + 3 * a] - elrayl[i + 3 * a];
             rhsid[i + 3 * p] += elrhs;
             if (finte) finte[i + 3 * p] += elfint[i + 3 * a];
             if (fexte) fexte[i + 3 * p] += elfext[i + 3 * a];
@@ -704,7 +725,14 @@ REAL FN(orc_critical_dt)(int nelem, const int32_t* lnods, const REAL* coord,
  *   Endste (sld_updunk.f90:149-185) state slot TIME_N <- ITER_K.
  * bcfun[ipoin] selects the table of a node's fixed dofs (-1: value 0);
  * fext_nodal is scaled by column 1 of table load_fun (-1: not applied).
- * wit_hist receives displ at the nwit witness dofs after every step. */
+ * wit_hist receives displ at the nwit witness dofs after every step.
+ * dampi (2, nmate, NULL: none): Rayleigh alpha damping with the velocity the
+ * reference holds in veloc(ITER_K) during the element loop -- the step-
+ * boundary velocity v_n in the central-difference scheme (written by the
+ * previous corrector, :201), the predicted v_n + dt a_n in Tchamwa-Wielgosz
+ * (:413).  The stiffness-proportional beta term (sld_elmmat.f90:170-190) is
+ * not restated: no reference deck sets RAYBETA and its term is marked for
+ * revision there; the CUDA library rejects beta > 0. */
 int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
                    const int32_t* lmate, const REAL* props, const REAL* e_mart,
                    const REAL* densi, const REAL* tempe, const int32_t* fixno,
@@ -715,7 +743,7 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
                    int nthreads, REAL dtime, int nsteps, REAL* cutim, REAL* displ,
                    REAL* veloc, REAL* accel, REAL* sdv, REAL* rhsid, int nwit,
                    const int32_t* wit_dof, REAL* wit_hist, int32_t* counters,
-                   int scheme, REAL phi)
+                   int scheme, REAL phi, const REAL* dampi)
 {
   int64_t ndof = 3 * (int64_t)npoin;
   REAL* vtmp = (REAL*)malloc(sizeof(REAL) * ndof);
@@ -757,7 +785,7 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
     FN(orc_assemble)(nelem, npoin, lnods, coord, displ, lmate, props, e_mart, densi, tempe,
                      NULL, (fext_nodal && load_fun >= 0) ? fext_nodal : NULL, scale, fixno,
                      sdv, ncolor, color_ptr, color_elem, nthreads, rhsid, NULL, NULL, NULL,
-                     vmass, &dmin, counters);
+                     vmass, &dmin, counters, dampi ? (scheme == 1 ? vtmp : veloc) : NULL, dampi);
     int nonfin = 0;
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(+ : nonfin)
     for (int p = 0; p < npoin; ++p) {

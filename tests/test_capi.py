@@ -42,6 +42,18 @@ def test_rejects_bad_material():
         sma.ExplicitSolid(p)
 
 
+def test_rejects_rayleigh_beta_and_negative_alpha():
+    """Stiffness-proportional (beta) damping is refused at the boundary rather
+    than ignored; alpha must be >= 0."""
+    import dataclasses
+    p = dataclasses.replace(_prob(), dampi=np.array([[0.0, 1e-6]]))
+    with pytest.raises(sma.SmaError, match="beta"):
+        sma.ExplicitSolid(p)
+    p = dataclasses.replace(_prob(), dampi=np.array([[-1.0, 0.0]]))
+    with pytest.raises(sma.SmaError, match="alpha"):
+        sma.ExplicitSolid(p)
+
+
 def test_rejects_bad_precision_and_block():
     p = _prob()
     with pytest.raises(KeyError):

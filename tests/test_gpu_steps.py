@@ -50,6 +50,53 @@ def test_tw_scheme_matches_oracle(oracle, bar):
     assert o.sdv[:, 1, :, 0].max() > 0.05
 
 
+@pytest.mark.parametrize("scheme", ["cd", "tw"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_rayleigh_alpha_damping_matches_oracle(oracle, bar, scheme, precision):
+    """RAYLEIGH_DAMPING RAYALPHA (sld_elmmat.f90:156-159): the element loop
+    subtracts alpha rho N v(g) dV with the velocity the reference's loop reads
+    (v_n in central differences, the predicted velocity in TW)."""
+    import dataclasses
+    p = dataclasses.replace(bar, dampi=np.array([[2.0e5, 0.0]]))
+    nsteps = 300
+    mid = int(np.argmin(np.sum((p.coord - [20, 2, 2]) ** 2, axis=1)))
+    wit = [3 * mid, 3 * mid + 1]
+    o = oracle.Problem(p)
+    h_ref = o.run(p.dtime, nsteps, wit_dof=wit, scheme=scheme, phi=1.033)
+    g = sma.ExplicitSolid(p, precision=precision, scheme=scheme, phitw=1.033)
+    g.set_witness(wit, nsteps)
+    g.step(nsteps)
+    h = g.witness()
+    tol = 1e-6 if precision == "fp64" else 5e-4
+    assert np.abs(h - h_ref).max() / np.abs(h_ref).max() < tol
+    assert np.abs(g.get("veloc") - o.veloc).max() / np.abs(o.veloc).max() < 10 * tol
+    # the damping acts: the undamped run keeps more kinetic energy
+    u = oracle.Problem(bar)
+    u.run(bar.dtime, nsteps, scheme=scheme, phi=1.033)
+    assert np.sum(o.veloc ** 2) < 0.5 * np.sum(u.veloc ** 2)
+
+
+def test_rayleigh_assemble_keeps_damping_out_of_finte(oracle, bar):
+    """sma_assemble with damping: rhsid and frxid carry the Rayleigh force,
+    finte and fexte do not (sld_elmmat.f90:168, sld_element_operations)."""
+    import dataclasses
+    p = dataclasses.replace(bar, dampi=np.array([[3.0e5, 0.0]]))
+    rng = np.random.default_rng(7)
+    u = rng.normal(size=(p.npoin, 3)) * 1e-3
+    v = rng.normal(size=(p.npoin, 3)) * 1e3
+    g = sma.ExplicitSolid(p, precision="fp64", scatter="color")
+    g.set("veloc", v)
+    got = g.assemble(u)
+    o = oracle.Problem(p)
+    ref = o.assemble(u, veloc=v)
+    for k in ("rhsid", "finte", "fexte", "frxid"):
+        scale = max(np.abs(ref[k]).max(), 1e-30)
+        assert np.abs(got[k] - ref[k]).max() <= 1e-8 * scale + 1e-300, k
+    und = oracle.Problem(bar).assemble(u)
+    assert np.abs(ref["finte"] - und["finte"]).max() <= 1e-12 * np.abs(und["finte"]).max()
+    assert np.abs(ref["rhsid"] - und["rhsid"]).max() > 1e-3 * np.abs(und["rhsid"]).max()
+
+
 def _funbou(oracle, tab, smooth, t):
     fn = oracle.lib().orc_funbou_f64
     fn.restype = C.c_double
@@ -58,11 +105,15 @@ def _funbou(oracle, tab, smooth, t):
     return fn(tb.shape[0], tb.ctypes.data_as(C.POINTER(C.c_double)), int(smooth), 0, float(t))
 
 
-def test_energy_balance_matches_restatement(oracle, canti):
+@pytest.mark.parametrize("alpha", [0.0, 1.0e5])
+def test_energy_balance_matches_restatement(oracle, canti, alpha):
     """ALLIE/ALLWK/ALLKE/ETOTA/EENER of mod_sld_energy.f90:71-193, computed by
     the device after every step, against the same formulas evaluated on
-    oracle step snapshots."""
-    p = canti
+    oracle step snapshots.  With Rayleigh damping the internal force of the
+    balance is finte, which leaves the damping force out as the reference's
+    does."""
+    import dataclasses
+    p = dataclasses.replace(canti, dampi=np.array([[alpha, 0.0]])) if alpha else canti
     nsteps = 200
     g = sma.ExplicitSolid(p, precision="fp64")
     g.set_energy(True, nsteps)
@@ -72,6 +123,7 @@ def test_energy_balance_matches_restatement(oracle, canti):
     o = oracle.Problem(p)
     vmass = o.assemble(np.zeros_like(o.displ))["vmass"]
     o.sdv[:] = 0.0
+    side = oracle.Problem(p)                                   # re-runs a step's element loop
     tab = p.fun_table(p.load_fun)
     allie = allwk = 0.0
     fint_prev = np.zeros_like(o.displ)
@@ -79,9 +131,14 @@ def test_energy_balance_matches_restatement(oracle, canti):
     ref = []
     for s in range(nsteps):
         u0 = o.displ.copy()
+        v0, sdv0 = o.veloc.copy(), o.sdv.copy()
         o.run(p.dtime, 1)
         fx = p.fext * _funbou(oracle, tab, p.fun_smooth[p.load_fun], o.cutim[0])
-        fi = fx - o.rhsid
+        if alpha:
+            side.sdv[:] = sdv0
+            fi = side.assemble(o.displ, veloc=v0)["finte"]
+        else:
+            fi = fx - o.rhsid
         dd = o.displ - u0
         ie = np.sum((fi + fint_prev) * dd)
         wk = np.sum((fx + fext_prev) * dd)
