@@ -255,6 +255,11 @@ struct sma_ctx {
   double* d_en = nullptr;                  // [4..8] totals (ALLIE, ALLWK, ALLKE, EENER, steps)
   double* d_epart = nullptr;               // per-block partial sums of the nodal kernel
   double* d_fray = nullptr;                // Rayleigh alpha nodal force (damped runs), SoA
+  // pipelined sma_assemble (atomic scatter, >= 2 slabs): slab bounds, node
+  // prefixes needed / finished per slab, copy streams and their events
+  std::vector<int> pl_e, pl_need, pl_final;
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  std::vector<cudaEvent_t> pl_ev;          // 2 K + 1
   double* d_ehist = nullptr;
   int* d_erow = nullptr;
   // host copies
@@ -390,6 +395,99 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
 int32_t launch_elements(sma_ctx* c, bool advance) {
   return c->prec == SMA_PREC_FP32 ? launch_elements_t<float>(c, advance)
                                   : launch_elements_t<double>(c, advance);
+}
+
+// one element range [beg, end) of an atomic-scatter context outside a step
+template <typename T>
+int32_t launch_element_range_t(sma_ctx* c, int beg, int end) {
+  if (end <= beg) return SMA_OK;
+  const int epb = c->block / 8;
+  ElemArgs<T> a = elem_args<T>(c, beg, end, false, false);
+  const int64_t ntiles = ceil_div(end - beg, epb);
+  const unsigned grid = c->variant == SMA_VARIANT_PIPE
+                            ? (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident)
+                            : (unsigned)ntiles;
+  elem_kernel<T>(c)<<<grid, c->block, elem_smem<T>(c), c->stream>>>(a);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+// Slab plan of the pipelined element-loop boundary (atomic scatter): K
+// element slabs; before slab s runs, nodes [0, need[s]) must be on the
+// device; after it, the residual of nodes [0, final[s]) is complete (no later
+// slab touches them).  Meshes numbered with locality (structured, O-grid,
+// concatenated specimens) give growing prefixes, so the copies in and out
+// overlap the element work; a mesh without it degrades to need = npoin.
+void plan_pipeline(sma_ctx* c, const int32_t* ln) {
+  const int K = (int)std::min<int64_t>(8, std::max<int64_t>(1, c->nelem / 16384));
+  c->pl_e.assign(K + 1, 0);
+  c->pl_need.assign(K, 0);
+  c->pl_final.assign(K, 0);
+  if (K < 2) return;
+  for (int s = 0; s <= K; ++s) c->pl_e[s] = (int)((int64_t)c->nelem * s / K);
+  std::vector<int8_t> last(c->npoin, -1);
+  int hi = 0;
+  for (int s = 0; s < K; ++s) {
+    for (int64_t k = 8 * (int64_t)c->pl_e[s]; k < 8 * (int64_t)c->pl_e[s + 1]; ++k) {
+      hi = std::max(hi, ln[k] + 1);
+      last[ln[k]] = (int8_t)s;
+    }
+    c->pl_need[s] = hi;
+  }
+  c->pl_need[K - 1] = c->npoin;                 // every node converted by the last slab
+  std::vector<int> first_bad(K, c->npoin);      // first node a later slab still touches
+  for (int p = c->npoin - 1; p >= 0; --p)
+    for (int s = 0; s < last[p]; ++s) first_bad[s] = p;
+  for (int s = 0; s < K; ++s) c->pl_final[s] = std::min(first_bad[s], c->pl_need[s]);
+  c->pl_final[K - 1] = c->npoin;
+}
+
+// sma_assemble's residual path, pipelined over the slab plan: H2D of the
+// node prefix a slab needs on one copy stream, conversion + element slab +
+// finished-node output on the context stream, D2H of finished nodes on a
+// second copy stream
+template <typename T>
+int32_t assemble_pipelined_t(sma_ctx* c, const double* displ, double scale, double* rhsid) {
+  const int K = (int)c->pl_need.size();
+  cudaEvent_t* ev_in = c->pl_ev.data();
+  cudaEvent_t* ev_out = c->pl_ev.data() + K;
+  cudaEvent_t ev_start = c->pl_ev[2 * K];
+  c->last_in = c->cur;
+  CU(cudaEventRecord(ev_start, c->stream));            // after all earlier work on the stream
+  CU(cudaStreamWaitEvent(c->s_h2d, ev_start, 0));
+  int64_t copied = 0, sent = 0;
+  const size_t row = 3 * sizeof(double);
+  for (int s = 0; s < K; ++s) {
+    const int64_t need = c->pl_need[s];
+    if (need > copied) {
+      CU(cudaMemcpyAsync(c->d_stage + 3 * copied, displ + 3 * copied, (need - copied) * row,
+                         cudaMemcpyHostToDevice, c->s_h2d));
+      CU(cudaEventRecord(ev_in[s], c->s_h2d));
+      CU(cudaStreamWaitEvent(c->stream, ev_in[s], 0));
+      k_assemble_in<<<(unsigned)ceil_div(need - copied, 256), 256, 0, c->stream>>>(
+          c->d_stage, c->d_u, c->d_f, c->d_fext, c->d_flags, scale, copied, need, c->npad);
+      c->launches++;
+      copied = need;
+    }
+    int32_t rc = launch_element_range_t<T>(c, c->pl_e[s], c->pl_e[s + 1]);
+    if (rc) return rc;
+    const int64_t fin = c->pl_final[s];
+    if (fin > sent) {
+      k_rhsid_out<<<(unsigned)ceil_div(fin - sent, 256), 256, 0, c->stream>>>(c->d_f, c->d_stage2, sent,
+                                                                              fin, c->npad);
+      c->launches++;
+      CU(cudaEventRecord(ev_out[s], c->stream));
+      CU(cudaStreamWaitEvent(c->s_d2h, ev_out[s], 0));
+      CU(cudaMemcpyAsync(rhsid + 3 * sent, c->d_stage2 + 3 * sent, (fin - sent) * row,
+                         cudaMemcpyDeviceToHost, c->s_d2h));
+      sent = fin;
+    }
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(c->s_d2h));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
 }
 
 // post-processing element pass reading state buffer `slot`
@@ -608,6 +706,9 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
                   c->d_pp_out, c->d_pp_gp, c->d_fray};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  for (cudaEvent_t e : c->pl_ev) cudaEventDestroy(e);
+  if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
+  if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SMA_OK;
@@ -721,6 +822,17 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
     std::memcpy(&lnods_i[8 * (size_t)e], mesh->lnods + 8 * (int64_t)c->perm[e], 8 * sizeof(int32_t));
   TRY(dalloc(&c->d_lnods, lnods_i.size() * sizeof(int32_t)));
   TRYCU(cudaMemcpy(c->d_lnods, lnods_i.data(), lnods_i.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (c->scatter == SMA_SCATTER_ATOMIC) {
+    plan_pipeline(c, lnods_i.data());
+    if (c->pl_need.size() >= 2) {
+      TRYCU(cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
+      TRYCU(cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
+      c->pl_ev.resize(2 * c->pl_need.size() + 1, nullptr);
+      for (cudaEvent_t& e : c->pl_ev) TRYCU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    } else {
+      c->pl_need.clear();                  // one slab: the serial path
+    }
+  }
   TRY(dalloc(&c->d_perm, c->perm.size() * sizeof(int32_t)));
   TRYCU(cudaMemcpy(c->d_perm, c->perm.data(), c->perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   if (mesh->lmate && c->nmate > 1) {
@@ -893,13 +1005,21 @@ int32_t sma_assemble(sma_ctx* c, const double* displ, double fext_scale, double*
   CU(cudaSetDevice(c->dev));
   const size_t bytes = 3 * (size_t)c->npoin * sizeof(double);
   const unsigned ngrid = (unsigned)ceil_div(c->npoin, 256);
-  CU(cudaMemcpyAsync(c->d_stage, displ, bytes, cudaMemcpyHostToDevice, c->stream));
-  k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_u, c->npoin, c->npad);
-  k_fill_f<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin, c->npad);
-  c->launches += 2;
-  CU(cudaGetLastError());
-  int32_t rc = launch_elements(c, false);
-  if (rc) return rc;
+  int32_t rc;
+  const bool piped = !c->pl_need.empty();
+  if (piped) {
+    // displacement in, element slabs and residual out overlapped
+    rc = c->prec == SMA_PREC_FP32 ? assemble_pipelined_t<float>(c, displ, fext_scale, rhsid)
+                                  : assemble_pipelined_t<double>(c, displ, fext_scale, rhsid);
+    if (rc) return rc;
+  } else {
+    CU(cudaMemcpyAsync(c->d_stage, displ, bytes, cudaMemcpyHostToDevice, c->stream));
+    k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_u, c->npoin, c->npad);
+    k_fill_f<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin, c->npad);
+    c->launches += 2;
+    CU(cudaGetLastError());
+    if ((rc = launch_elements(c, false))) return rc;
+  }
   double* outs[4] = {rhsid, finte, fexte, frxid};
   // with damping, finte leaves the Rayleigh force out (it is in rhsid only)
   const double* fray = nullptr;
@@ -907,7 +1027,7 @@ int32_t sma_assemble(sma_ctx* c, const double* displ, double fext_scale, double*
     if ((rc = launch_rayleigh(c, damp_velocity(c, false)))) return rc;
     fray = c->d_fray;
   }
-  for (int q = 0; q < 4; ++q) {
+  for (int q = piped ? 1 : 0; q < 4; ++q) {
     if (!outs[q]) continue;
     double* dr = c->d_stage;
     k_outputs<<<ngrid, 256, 0, c->stream>>>(c->d_f, c->d_fext, c->d_flags, fext_scale, c->npoin,

@@ -914,6 +914,27 @@ __global__ void k_fill_f(double* f, const double* fext, const uint8_t* flags, do
       f[k] = (fext && (flags[p] & 8u)) ? fext[k] * scale : 0.0;
     }
 }
+// pipelined element-loop boundary, nodes [p0, p1): displacement (3, npoin)
+// -> SoA, and the residual initialised with the scaled nodal load
+__global__ void k_assemble_in(const double* aos, double* u, double* f, const double* fext,
+                              const uint8_t* flags, double scale, int64_t p0, int64_t p1,
+                              int64_t npad) {
+  const int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= p1) return;
+  const bool loaded = fext && (flags[p] & 8u);
+  for (int c = 0; c < 3; ++c) {
+    const int64_t k = c * npad + p;
+    u[k] = aos[3 * p + c];
+    f[k] = loaded ? fext[k] * scale : 0.0;
+  }
+}
+// ... and the residual of nodes [p0, p1) back to (3, npoin)
+__global__ void k_rhsid_out(const double* f, double* aos, int64_t p0, int64_t p1, int64_t npad) {
+  const int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < p1)
+    for (int c = 0; c < 3; ++c) aos[3 * p + c] = f[c * npad + p];
+}
+
 // assemble outputs (3, npoin): rhsid, finte = fexte - rhsid, fexte (nodal
 // loads), frxid = element part of rhsid on prescribed dofs
 __global__ void k_outputs(const double* f, const double* fext, const uint8_t* flags,
