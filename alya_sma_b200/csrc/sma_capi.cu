@@ -872,7 +872,11 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   TRY(dalloc(&c->d_stage, 3 * (size_t)c->npoin * sizeof(double)));
   TRY(dalloc(&c->d_stage2, 3 * (size_t)c->npoin * sizeof(double)));
   const unsigned ngrid = (unsigned)ceil_div(c->npoin, 256);
-  TRYCU(cudaMemcpy(c->d_stage, mesh->coord, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyHostToDevice));
+  // staged uploads are ordered on the context stream: the staging buffer is
+  // reused, and a blocking copy does not wait for kernels on a non-blocking
+  // stream that still read the previous contents
+  TRYCU(cudaMemcpyAsync(c->d_stage, mesh->coord, 3 * (size_t)c->npoin * sizeof(double),
+                        cudaMemcpyHostToDevice, c->stream));
   k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_coord, c->npoin, c->npad);
   TRYCU(cudaGetLastError());
 
@@ -892,7 +896,8 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
         flags[p] |= 8u;
     TRY(dalloc(&c->d_fext, nb));
     TRYCU(cudaMemset(c->d_fext, 0, nb));
-    TRYCU(cudaMemcpy(c->d_stage, run->fext, 3 * (size_t)c->npoin * sizeof(double), cudaMemcpyHostToDevice));
+    TRYCU(cudaMemcpyAsync(c->d_stage, run->fext, 3 * (size_t)c->npoin * sizeof(double),
+                          cudaMemcpyHostToDevice, c->stream));
     k_aos_to_soa<<<ngrid, 256, 0, c->stream>>>(c->d_stage, c->d_fext, c->npoin, c->npad);
     TRYCU(cudaGetLastError());
   }
@@ -1228,6 +1233,7 @@ int32_t sma_get_witness(sma_ctx* c, double* host, int32_t* nsteps_out) {
   if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
   if (c->nwit <= 0) return fail(SMA_ERR_STATE, "no witnesses set");
   CU(cudaSetDevice(c->dev));
+  CU(cudaStreamSynchronize(c->stream));    // the witness kernels run on the context stream
   int rows = 0;
   CU(cudaMemcpy(&rows, c->d_wrow, sizeof(int), cudaMemcpyDeviceToHost));
   rows = std::min(rows, c->wit_max);

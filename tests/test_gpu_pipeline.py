@@ -63,6 +63,21 @@ def _compare(pa, ua, pb, ub, map_nodes=None, map_elems=None):
         b.end_step()
 
 
+@pytest.mark.parametrize("scatter", ["atomic", "color"])
+def test_large_mesh_assemble_matches_oracle(oracle, canti, scatter):
+    """80k elements with a traction load: every output against the oracle.
+    (Context set-up stages coordinates and loads through one buffer; an
+    upload that is not ordered behind the previous conversion kernel shows
+    up here as coordinates read as loads.)"""
+    u = _field(canti, 0)
+    g = sma.ExplicitSolid(canti, precision="fp64", scatter=scatter)
+    got = g.assemble(u, fext_scale=0.5)
+    ref = oracle.Problem(canti).assemble(u, fext_scale=0.5)
+    for k in ("rhsid", "finte", "fexte", "frxid"):
+        scale = max(np.abs(ref[k]).max(), 1e-30)
+        assert np.abs(got[k] - ref[k]).max() <= 1e-8 * scale, k
+
+
 def test_pipelined_assemble_equals_serial(canti):
     u = [_field(canti, 0), _field(canti, 1)]
     _compare(canti, u, canti, u)
