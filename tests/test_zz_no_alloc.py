@@ -70,7 +70,9 @@ def test_noalloc_matches_context_entry_point(precision):
         assert err < tol, (call, err)
         st = sdv.cpu().numpy()
         st_ref = ref.state                                  # after end_step: slot 1 = TIME_N
-        assert np.abs(st[:, 0] - st_ref[:, 1]).max() < (1e-9 if precision == "fp64" else 1e-4)
+        # relative to the largest state value (the F_AS/F_SA entries are ~1e2)
+        srel = np.abs(st[:, 0] - st_ref[:, 1]).max() / np.abs(st_ref[:, 1]).max()
+        assert srel < (1e-11 if precision == "fp64" else 1e-5), (call, srel)
         sdv[:, 1] = sdv[:, 0]                               # end of step: TIME_N <- ITER_K
     assert st[:, 0, :, 0].max() > 0.05                      # martensite formed
     ref.close()
