@@ -187,7 +187,7 @@ __device__ __forceinline__ void lds8(const double* p, double* v) {
 // drops out), Ji = J^-1 (Ji[3j+k] = dxi_j/dX_k) and H = dU/dX = Gu Ji
 // (jacobi.f90:172-219, sld_elmpre.f90:149-162).  Returns det J.
 template <typename T>
-__device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H) {
+__device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H, T* Jc = nullptr) {
   T J[9], Gu[9];
   {
     // this lane's Gauss point: derivatives in registers (a table row per
@@ -215,6 +215,9 @@ __device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H) {
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
+  if (Jc)                                                        // F J = dx/dxi = J + Gu
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Jc[k] = J[k] + Gu[k];
   return detJ;
 }
 
@@ -243,8 +246,8 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   __syncwarp();                                                  // node rows of the element
 
   // ---- phase 1, lane = Gauss point g ------------------------------------
-  T Ji[9], H[9];
-  const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H);
+  T Ji[9], H[9], Jc[9];                                          // Jc = F J, live across the law
+  const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H, Jc);
 
   // ---- constitutive update ----------------------------------------------
   T tau[6];
@@ -256,17 +259,8 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   }
 
   // ---- force operator Q = vol tau (F J)^-T, f_a = -Q dN_a ---------------
-  T Fm[9], Fi[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) Fm[k] = H[k];
-  Fm[0] += T(1); Fm[4] += T(1); Fm[8] += T(1);
-  const T detF = inv3(Fm, Fi);
-  T B[9];                                                        // B = Ji Fi = (F J)^-1
-#pragma unroll
-  for (int m = 0; m < 3; ++m)
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      B[3 * m + k] = Ji[3 * m + 0] * Fi[0 + k] + Ji[3 * m + 1] * Fi[3 + k] + Ji[3 * m + 2] * Fi[6 + k];
+  T B[9];                                                        // B = (F J)^-1 = dxi/dx
+  const T detFJ = inv3(Jc, B);                                   // det F = det(F J) / det J
   const T vol = detJ;                                            // Gauss weight 1
   const T t00 = tau[0] * vol, t11 = tau[1] * vol, t22 = tau[2] * vol;
   const T t01 = tau[3] * vol, t12 = tau[4] * vol, t02 = tau[5] * vol;
@@ -337,9 +331,14 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
     }
   }
   count_warp(a.cnt, CNT_NR_ACTIVE, valid && (flag & (NR_CONVERGED | NR_FAILED)));
-  count_warp(a.cnt, CNT_NR_FAILED, valid && (flag & NR_FAILED));
-  count_warp(a.cnt, CNT_NR_BOTH, valid && (flag & NR_BOTH));
-  count_warp(a.cnt, CNT_NEG_DET, valid && !(detF > T(0)));
+  // the rare events behind one vote: failed return map, both transformations,
+  // det F <= 0 (det F = det(F J) / det J)
+  const bool negdet = !(detFJ * detJ > T(0));
+  if (__any_sync(0xffffffffu, valid && ((flag & (NR_FAILED | NR_BOTH)) || negdet))) {
+    count_warp(a.cnt, CNT_NR_FAILED, valid && (flag & NR_FAILED));
+    count_warp(a.cnt, CNT_NR_BOTH, valid && (flag & NR_BOTH));
+    count_warp(a.cnt, CNT_NEG_DET, valid && negdet);
+  }
 }
 
 // a material is copied as MAT_CHUNKS 16-byte chunks by the 8 lanes of its element
