@@ -12,9 +12,11 @@ accumulation and integration); the plain FP64 form is timed beside it.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp64] [--scatter atomic|color]
 
---gpus N > 1 (under torchrun): each rank runs an independent specimen of
-the same workload (the batched-ensemble partition: specimens shard across
-GPUs with no exchange), weak scaling, max over ranks of the device time.
+--gpus N > 1 (under torchrun): the cantilever and cylinder run one
+independent replica per rank (weak scaling); --workload ensemble shards its
+256 specimens across the ranks, largest first onto the least loaded rank,
+with no exchange (strong scaling).  Either way the time is the maximum over
+ranks of the device time and `value` counts every rank's Gauss points.
 --impl reference times the CPU restatement of the reference path (the
 oracle: the reference is Fortran and cannot be built here) on the host
 cores of rank 0, on a bounded sample of the same workload.
@@ -157,12 +159,20 @@ def algorithmic_bytes(prob, precision):
     return prob.nelem * (32 + 2 * 8 * 3 * s) + prob.npoin * (24 + 24 + 48)
 
 
-def build_problem(workload, div):
+def build_problem(workload, div, rank=0, world=1):
+    """The workload's mesh on this rank.  The ensemble shards its specimens
+    across ranks (largest first onto the least loaded rank); the other
+    workloads run one replica per rank."""
     from alya_sma_b200 import problem as P
     if workload == "cylinder":
         return P.cylinder_2m(nsteps=10000, div=div)
     if workload == "ensemble":
-        return P.ensemble(nspec=max(2, 256 // div), nsteps=5000)
+        nspec = max(2, 256 // div)
+        if world > 1:
+            from alya_sma_b200 import dist as D
+            mine = D.shard_specimens(P.ensemble_sizes(nspec), rank, world)
+            return P.ensemble(nspec=nspec, nsteps=5000, subset=mine)
+        return P.ensemble(nspec=nspec, nsteps=5000)
     return P.cantilever_400x40x40(nsteps=20000, div=div)
 
 
@@ -221,8 +231,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    prob = build_problem(args.workload, args.div)
+    prob = build_problem(args.workload, args.div, rank, world)
     nelem, ngp = prob.nelem, prob.nelem * 8
+    sharded = args.workload == "ensemble" and world > 1       # strong scaling: fixed total work
 
     from alya_sma_b200 import problem as P
     u0 = P.prestrain(prob, args.prestrain)
@@ -266,11 +277,13 @@ def main():
     ck = clocks.stop()
     launches = solid.kernel_launches - l0
     ms = e0.elapsed_time(e1)
+    ngp_all = world * ngp                                      # replicas: the same mesh per rank
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * ngp * args.steps / (ms / 1e3)
+        from alya_sma_b200 import dist as D
+        ms = D.max_over_ranks(ms, "cuda")                      # the slowest rank sets the time
+        if sharded:
+            ngp_all = int(D.sum_over_ranks(ngp, "cuda"))       # each specimen counted once
+    value = ngp_all * args.steps / (ms / 1e3)
 
     # ---- per-kernel device times (roofline of the element kernel): the same
     # K steps replayed from the checkpoint, CUDA events around every launch
@@ -355,16 +368,18 @@ def main():
         line = {"metric": "Gauss-point updates/s (explicit SMA step)", "value": value,
                 "unit": "GP-updates/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
+                "scaling": "strong" if sharded else "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if args.precision == "fp32" else "f64",
                 "data": "synthetic",
                 "config": {"workload": WORKLOADS[args.workload], "nelem": nelem, "npoin": prob.npoin,
-                           "gauss_points": ngp, "precision": args.precision,
-                           "scatter": args.scatter, "block": block or (256 if args.precision == "fp32" else 128), "variant": variant, "autotuned": bool(tuned), "dtime": prob.dtime,
+                           "gauss_points": ngp_all, "precision": args.precision,
+                           "scatter": args.scatter, "block": block or 128, "variant": variant,
+                           "autotuned": bool(tuned), "dtime": prob.dtime,
                            "prestrain": args.prestrain,
                            "l2": "working set > L2 (state, nodal arrays and connectivity "
                                  f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                           "parallelism": (f"specimens sharded over {world} GPUs (no exchange)" if sharded
+                                           else f"replicas x{world}" if world > 1 else "single GPU")},
                 "roofline": roofline, "gpu_launches": launches, "clocks": ck}
         line.update(extras)
         print(json.dumps(line))
