@@ -63,7 +63,7 @@ VARIANT = {"auto": 0, "pipe": 1, "plain": 2}
 
 
 class _Counters(C.Structure):
-    _fields_ = [("c", C.c_int64 * 8), ("gpdet_min", C.c_double)]
+    _fields_ = [("c", C.c_int64 * 8), ("gpdet_min", C.c_double), ("ielem_min", C.c_int64)]
 
 
 _lib = None
@@ -95,6 +95,7 @@ def lib():
         L.sma_assemble_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
         L.sma_end_step.argtypes = [C.c_void_p]
         L.sma_postprocess.argtypes = [C.c_void_p] * 6
+        L.sma_gauss_fields.argtypes = [C.c_void_p] * 5
         L.sma_eval_law160.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p]
@@ -252,7 +253,22 @@ class ExplicitSolid:
         _check(lib().sma_get_counters(self._ctx, C.byref(c)))
         if reset:
             _check(lib().sma_reset_counters(self._ctx))
-        return {name: int(c.c[i]) for i, name in enumerate(COUNTERS)}
+        out = {name: int(c.c[i]) for i, name in enumerate(COUNTERS)}
+        out["gpdet_min"] = float(c.gpdet_min)                 # smallest det F <= 0, 0.0 if none
+        out["ielem_min"] = int(c.ielem_min)                   # its element, -1 if none
+        return out
+
+    def gauss_fields(self):
+        """Element-loop fields per Gauss point from the same evaluation as
+        postprocess(): 'gpgdi' (F) and 'gppio' (P = F S) as (nelem, 8, 3, 3)
+        holding Fortran T(i,j) at [..., j, i], 'gpdet' (nelem, 8) and
+        'volum' = (reference volume, deformed volume)."""
+        out = {k: np.zeros((self.nelem, 8, 3, 3)) for k in ("gpgdi", "gppio")}
+        out["gpdet"] = np.zeros((self.nelem, 8))
+        out["volum"] = np.zeros(2)
+        _check(lib().sma_gauss_fields(self._ctx, _p(out["gpgdi"]), _p(out["gppio"]), _p(out["gpdet"]),
+                                      _p(out["volum"])))
+        return out
 
     def set_witness(self, dofs, max_steps):
         d = np.ascontiguousarray(dofs, dtype=np.int32)

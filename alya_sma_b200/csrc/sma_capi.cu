@@ -234,6 +234,10 @@ struct sma_ctx {
   double* d_pp_acc = nullptr;              // post-processing: [19][npad] nodal sums
   double* d_pp_out = nullptr;              //   (19, npoin) nodal results
   double* d_pp_gp = nullptr;               //   (6, 8, nelem) Gauss-point Cauchy stress
+  double* d_gp_F = nullptr;                // sma_gauss_fields: gpgdi, gppio (72 nelem),
+  double* d_gp_P = nullptr;                //   det F (8 nelem), volumes (2)
+  double* d_gp_det = nullptr;
+  double* d_gp_vol = nullptr;
   unsigned long long* d_cnt = nullptr;
   StepTime* d_ts = nullptr;
   FunTab* d_ft = nullptr;
@@ -490,15 +494,14 @@ int32_t assemble_pipelined_t(sma_ctx* c, const double* displ, double scale, doub
   return SMA_OK;
 }
 
-// post-processing element pass reading state buffer `slot`
+// post-processing element pass: the law from the state the last element
+// loop read (TIME_N if none ran since the state was set), outputs in p
 template <typename T>
-int32_t launch_postproc_t(sma_ctx* c, int slot) {
+int32_t launch_postproc_t(sma_ctx* c, PostArgs p) {
+  const int slot = c->last_in >= 0 ? c->last_in : c->cur;
   ElemArgs<T> a = elem_args<T>(c, 0, c->nelem, false);
   a.sold = (const T*)c->d_state[slot];
   a.snew = nullptr;
-  PostArgs p;
-  p.acc = c->d_pp_acc;
-  p.gp_sig = c->d_pp_gp;
   p.perm = c->d_perm;
   const int block = 128;
   const bool mats = c->d_lmate != nullptr;
@@ -703,7 +706,8 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
                   c->d_fextp, c->d_en, c->d_ehist, c->d_erow, c->d_epart, c->d_pp_acc,
-                  c->d_pp_out, c->d_pp_gp, c->d_fray};
+                  c->d_pp_out, c->d_pp_gp, c->d_fray, c->d_gp_F, c->d_gp_P, c->d_gp_det,
+                  c->d_gp_vol};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->pl_ev) cudaEventDestroy(e);
@@ -921,6 +925,7 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   TRY(c->prec == SMA_PREC_FP32 ? init_element_launch_t<float>(c) : init_element_launch_t<double>(c));
   TRY(dalloc(&c->d_cnt, NCNT * sizeof(unsigned long long)));
   TRYCU(cudaMemset(c->d_cnt, 0, NCNT * sizeof(unsigned long long)));
+  TRYCU(cudaMemset(c->d_cnt + CNT_DETMIN, 0xff, sizeof(unsigned long long)));   // none seen
 
   // time functions and step time
   FunTab ft;
@@ -1063,12 +1068,11 @@ int32_t sma_postprocess(sma_ctx* c, double* caust, double* green, double* lepsi,
   if (!c->d_pp_out && (rc = dalloc(&c->d_pp_out, PP_COLS * (size_t)c->npoin * sizeof(double)))) return rc;
   if (gp_sigma && !c->d_pp_gp && (rc = dalloc(&c->d_pp_gp, 48 * (size_t)c->nelem * sizeof(double))))
     return rc;
-  double* gp_keep = c->d_pp_gp;
-  if (!gp_sigma) c->d_pp_gp = nullptr;                          // the kernel skips the per-GP output
-  const int slot = c->last_in >= 0 ? c->last_in : c->cur;
+  PostArgs p{};
+  p.acc = c->d_pp_acc;
+  p.gp_sig = gp_sigma ? c->d_pp_gp : nullptr;                  // the kernel skips what is null
   CU(cudaMemsetAsync(c->d_pp_acc, 0, PP_COLS * (size_t)c->npad * sizeof(double), c->stream));
-  rc = c->prec == SMA_PREC_FP32 ? launch_postproc_t<float>(c, slot) : launch_postproc_t<double>(c, slot);
-  c->d_pp_gp = gp_keep;
+  rc = c->prec == SMA_PREC_FP32 ? launch_postproc_t<float>(c, p) : launch_postproc_t<double>(c, p);
   if (rc) return rc;
   k_postproc_nodal<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(c->d_pp_acc, c->npad,
                                                                              c->npoin, c->d_pp_out);
@@ -1086,6 +1090,32 @@ int32_t sma_postprocess(sma_ctx* c, double* caust, double* green, double* lepsi,
   if (gp_sigma)
     CU(cudaMemcpyAsync(gp_sigma, c->d_pp_gp, 48 * (size_t)c->nelem * sizeof(double),
                        cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_gauss_fields(sma_ctx* c, double* gpgdi, double* gppio, double* gpdet, double* volum) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc;
+  const size_t n72 = 72 * (size_t)c->nelem, n8 = 8 * (size_t)c->nelem;
+  // device buffers only for what is asked, kept for the next call
+  if (gpgdi && !c->d_gp_F && (rc = dalloc(&c->d_gp_F, n72 * sizeof(double)))) return rc;
+  if (gppio && !c->d_gp_P && (rc = dalloc(&c->d_gp_P, n72 * sizeof(double)))) return rc;
+  if (gpdet && !c->d_gp_det && (rc = dalloc(&c->d_gp_det, n8 * sizeof(double)))) return rc;
+  if (volum && !c->d_gp_vol && (rc = dalloc(&c->d_gp_vol, 2 * sizeof(double)))) return rc;
+  PostArgs p{};
+  p.gp_F = gpgdi ? c->d_gp_F : nullptr;
+  p.gp_P = gppio ? c->d_gp_P : nullptr;
+  p.gp_det = gpdet ? c->d_gp_det : nullptr;
+  p.volum = volum ? c->d_gp_vol : nullptr;
+  if (volum) CU(cudaMemsetAsync(c->d_gp_vol, 0, 2 * sizeof(double), c->stream));
+  rc = c->prec == SMA_PREC_FP32 ? launch_postproc_t<float>(c, p) : launch_postproc_t<double>(c, p);
+  if (rc) return rc;
+  if (gpgdi) CU(cudaMemcpyAsync(gpgdi, c->d_gp_F, n72 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (gppio) CU(cudaMemcpyAsync(gppio, c->d_gp_P, n72 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (gpdet) CU(cudaMemcpyAsync(gpdet, c->d_gp_det, n8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (volum) CU(cudaMemcpyAsync(volum, c->d_gp_vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
   return SMA_OK;
 }
@@ -1195,8 +1225,21 @@ int32_t sma_get_counters(sma_ctx* c, sma_counters* out) {
   unsigned long long h[NCNT];
   CU(cudaMemcpyAsync(h, c->d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k < NCNT) ? (int64_t)h[k] : 0;
-  out->gpdet_min = 0.0;
+  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k < CNT_DETMIN) ? (int64_t)h[k] : 0;
+  // the smallest det F <= 0 seen and its element (caller's numbering)
+  const unsigned long long dm = h[CNT_DETMIN];
+  if (dm == ~0ull) {
+    out->gpdet_min = 0.0;
+    out->ielem_min = -1;
+  } else {
+    const unsigned key = (unsigned)(dm >> 32);
+    const unsigned bits = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+    float det;
+    std::memcpy(&det, &bits, sizeof det);
+    out->gpdet_min = det;
+    const int64_t e = (int64_t)(dm & 0xffffffffull);
+    out->ielem_min = (e >= 0 && e < c->nelem) ? c->perm[e] : -1;
+  }
   return SMA_OK;
 }
 
@@ -1204,6 +1247,7 @@ int32_t sma_reset_counters(sma_ctx* c) {
   if (!c) return fail(SMA_ERR_ARG, "NULL context");
   CU(cudaSetDevice(c->dev));
   CU(cudaMemsetAsync(c->d_cnt, 0, NCNT * sizeof(unsigned long long), c->stream));
+  CU(cudaMemsetAsync(c->d_cnt + CNT_DETMIN, 0xff, sizeof(unsigned long long), c->stream));
   CU(cudaStreamSynchronize(c->stream));
   return SMA_OK;
 }

@@ -24,7 +24,17 @@ constexpr int MAXFUN = 16;
 constexpr int MAXPTS = 32;
 
 enum Cnt { CNT_NR_ACTIVE = 0, CNT_NR_FAILED, CNT_NR_BOTH, CNT_NEG_DET, CNT_NONFINITE,
-           CNT_FALLBACK64, NCNT = 8 };
+           CNT_FALLBACK64, CNT_DETMIN, NCNT = 8 };
+
+// CNT_DETMIN holds min over Gauss points with det F <= 0 of (det F, element)
+// packed for one 64-bit atomicMin: the float's bits mapped to an unsigned
+// key in the same order, then the internal element index; all ones = none
+// (sld_elmpre.f90:229-238, gpdet_min / ielem_min).
+__device__ __forceinline__ unsigned long long detmin_key(float det, int64_t e) {
+  const unsigned b = __float_as_uint(det);
+  const unsigned k = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  return ((unsigned long long)k << 32) | (unsigned long long)(unsigned)e;
+}
 
 // DISCRETE time functions (tload_sld tables), rows (t, vx, vy, vz)
 struct FunTab {
@@ -338,6 +348,7 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
     count_warp(a.cnt, CNT_NR_FAILED, valid && (flag & NR_FAILED));
     count_warp(a.cnt, CNT_NR_BOTH, valid && (flag & NR_BOTH));
     count_warp(a.cnt, CNT_NEG_DET, valid && negdet);
+    if (valid && negdet) atomicMin(a.cnt + CNT_DETMIN, detmin_key((float)(detFJ / detJ), ec));
   }
 }
 
@@ -570,8 +581,12 @@ constexpr int PP_COLS = 19;
 constexpr int PP_ROW = 20;                 // doubles per Gauss-point row (16-byte multiple)
 
 struct PostArgs {
-  double* acc;                             // [PP_COLS][npad]
+  double* acc;                             // [PP_COLS][npad], or null: no nodal sums
   double* gp_sig;                          // (6, 8, nelem) or null
+  double* gp_F;                            // gpgdi (3, 3, 8, nelem) column-major, or null
+  double* gp_P;                            // gppio (3, 3, 8, nelem) column-major, or null
+  double* gp_det;                          // det F (8, nelem), or null
+  double* volum;                           // [2] += (dV, dV det F) (volum_sld), or null
   const int32_t* perm;                     // internal element -> caller's element
 };
 
@@ -671,10 +686,43 @@ __global__ void __launch_bounds__(128) k_postproc(ElemArgs<T> a, PostArgs p) {
 #pragma unroll
     for (int v = 0; v < 6; ++v) o[v] = sig[v];
   }
+  // element-loop fields: F, P = tau F^-T (sld_builtin_materials.f90:362-371),
+  // det F (sld_elmpre.f90:217-226), column-major per Gauss point
+  if ((p.gp_F || p.gp_P || p.gp_det) && valid) {
+    const int64_t o9 = 9 * (8 * (int64_t)p.perm[ec] + lane8);
+    T Fm[9], Fi[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Fm[k] = H[k];
+    Fm[0] += T(1); Fm[4] += T(1); Fm[8] += T(1);
+    inv3(Fm, Fi);
+    const T tf[9] = {tau[0], tau[3], tau[5], tau[3], tau[1], tau[4], tau[5], tau[4], tau[2]};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        if (p.gp_F) p.gp_F[o9 + i + 3 * j] = (double)Fm[3 * i + j];
+        if (p.gp_P)
+          p.gp_P[o9 + i + 3 * j] = (double)(tf[3 * i + 0] * Fi[3 * j + 0] + tf[3 * i + 1] * Fi[3 * j + 1] +
+                                            tf[3 * i + 2] * Fi[3 * j + 2]);
+      }
+    if (p.gp_det) p.gp_det[8 * (int64_t)p.perm[ec] + lane8] = (double)detF;
+  }
+  if (p.volum) {                                                 // warp sums, one atomic per warp
+    double v0 = valid ? dv : 0.0, v1 = valid ? dv * (double)detF : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+      v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(p.volum, v0);
+      atomicAdd(p.volum + 1, v1);
+    }
+  }
   __syncwarp();
 
   // lane = node a: sum over the element's Gauss points
-  if (valid) {
+  if (valid && p.acc) {
 #pragma unroll 1
     for (int k = 0; k < PP_COLS; ++k) {
       double s = 0.0;

@@ -113,7 +113,14 @@ typedef struct {
 #define SMA_SCHEME_CD       0   /* central difference, mod_sld_solution_methods.f90:101-223 */
 #define SMA_SCHEME_TW       1   /* Tchamwa-Wielgosz, mod_sld_solution_methods.f90:385-574   */
 
-typedef struct { int64_t c[SMA_NCOUNTERS]; double gpdet_min; } sma_counters;
+/* gpdet_min / ielem_min: the smallest det F <= 0 met by an element loop since
+ * creation or reset (single precision) and its element in the caller's
+ * numbering; 0.0 / -1 when none (sld_elmpre.f90:229-238) */
+typedef struct {
+  int64_t c[SMA_NCOUNTERS];
+  double gpdet_min;
+  int64_t ielem_min;
+} sma_counters;
 
 /* Context: copies the host arrays to the device and owns every device buffer.
  * Replaces the reference's Begrun-time set-up of solidz (sld_inivar, mass) */
@@ -199,6 +206,13 @@ int32_t sma_get_time(sma_ctx* ctx, double* cutim);
 int32_t sma_set_time(sma_ctx* ctx, double cutim);
 int32_t sma_get_counters(sma_ctx* ctx, sma_counters* out);
 int32_t sma_reset_counters(sma_ctx* ctx);
+/* Element-loop fields per Gauss point, HOST buffers, any of them NULL, from
+ * the same evaluation as sma_postprocess: gpgdi = F and gppio = P = F S
+ * (3,3,8,nelem) column-major, gpdet = det F (8,nelem), volum[2] = (reference
+ * volume, deformed volume) summed over the mesh.  Replaces gpgdi_sld,
+ * gppio_sld, dedef_sld and volum_sld(1:2) (sld_elmpre.f90:217-264,
+ * sld_builtin_materials.f90:362-371). */
+int32_t sma_gauss_fields(sma_ctx* ctx, double* gpgdi, double* gppio, double* gpdet, double* volum);
 /* witness dofs: flat ids 3*p+i record the displacement of dof i of node p
  * after each step of the next sma_explicit_step call, ids 3*npoin + 3*p+i
  * its residual (f_ext - f_int; on prescribed dofs the reaction, as

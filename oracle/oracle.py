@@ -201,27 +201,35 @@ class Problem:
         out["gpdet_min"] = float(dmin[0])
         return out
 
-    def postprocess(self, displ=None, slot=1, gp_sigma=False):
+    def postprocess(self, displ=None, slot=1, gp_sigma=False, gauss=False):
         """Nodal Cauchy stress, Green and log strain (npoin, 6) in Voigt order
         xx yy zz yz xz xy, von Mises (npoin,), and optionally the Gauss-point
         Cauchy stress (nelem, 8, 6), with the law evaluated on state `slot`
-        (1 = TIME_N, what the last assemble() started from)."""
+        (1 = TIME_N, what the last assemble() started from).  gauss=True adds
+        the element-loop fields gpgdi / gppio (nelem, 8, 3, 3) holding
+        Fortran T(i,j) at [..., j, i], gpdet (nelem, 8) and volum (2,)."""
         ct = self.ct
         d = self.displ if displ is None else np.ascontiguousarray(displ, dtype=self.dtype)
         out = {k: np.zeros((self.npoin, 6), self.dtype) for k in ("caust", "green", "lepsi")}
         out["seqvm"] = np.zeros(self.npoin, self.dtype)
         gp = np.zeros((self.nelem, 8, 6), self.dtype) if gp_sigma else None
+        gf = {k: np.zeros((self.nelem, 8, 3, 3), self.dtype) for k in ("gpgdi", "gppio")} if gauss else {}
+        gdet = np.zeros((self.nelem, 8), self.dtype) if gauss else None
+        vol = np.zeros(2, self.dtype) if gauss else None
         fn = getattr(lib(), "orc_postprocess" + self.sfx)
         fn.argtypes = None
         rc = fn(self.nelem, self.npoin, _ptr(self.lnods, C.c_int32), _ptr(self.coord, ct),
                 _ptr(d, ct), _ptr(self.lmate, C.c_int32), _ptr(self.props, ct),
                 _ptr(self.e_mart, ct), _ptr(self.tempe, ct), _ptr(self.sdv, ct), int(slot),
                 _ptr(out["caust"], ct), _ptr(out["green"], ct), _ptr(out["lepsi"], ct),
-                _ptr(out["seqvm"], ct), _ptr(gp, ct))
+                _ptr(out["seqvm"], ct), _ptr(gp, ct), _ptr(gf.get("gpgdi"), ct),
+                _ptr(gf.get("gppio"), ct), _ptr(gdet, ct), _ptr(vol, ct))
         if rc:
             raise MemoryError("orc_postprocess")
         if gp_sigma:
             out["gp_sigma"] = gp
+        if gauss:
+            out.update(gf, gpdet=gdet, volum=vol)
         return out
 
     def end_step(self):

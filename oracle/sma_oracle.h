@@ -92,7 +92,8 @@ extern "C" {
   int  orc_postprocess##S(int nelem, int npoin, const int32_t* lnods, const T* coord,\
                           const T* displ, const int32_t* lmate, const T* props,     \
                           const T* e_mart, const T* tempe, const T* sdv, int slot,  \
-                          T* caust, T* green, T* lepsi, T* seqvm, T* gp_sigma);
+                          T* caust, T* green, T* lepsi, T* seqvm, T* gp_sigma,      \
+                          T* gp_F, T* gp_P, T* gp_det, T* volum);
 
 ORC_DECL(double, _f64)
 ORC_DECL(float, _f32)

@@ -832,13 +832,18 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
 /* on the state slot `slot` of sdv (its new state is discarded), as the       */
 /* element loop that produced gppio.  Voigt order xx yy zz yz xz xy           */
 /* (nvgij_sld, sld_inivar.f90:568-579).  Outputs are (6, npoin) except seqvm  */
-/* (npoin) and gp_sigma (6, 8, nelem); any output may be NULL.                */
+/* (npoin) and gp_sigma (6, 8, nelem); any output may be NULL.  The element-  */
+/* loop fields of the same evaluation: gp_F = gpgdi and gp_P = gppio          */
+/* (3, 3, 8, nelem) column-major, gp_det = det F (8, nelem), and volum[2] =   */
+/* (sum dV, sum dV det F) as volum_sld (sld_elmpre.f90:242-264).             */
 /* ------------------------------------------------------------------------ */
 int FN(orc_postprocess)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
                         const REAL* displ, const int32_t* lmate, const REAL* props,
                         const REAL* e_mart, const REAL* tempe, const REAL* sdv, int slot,
-                        REAL* caust, REAL* green, REAL* lepsi, REAL* seqvm, REAL* gp_sigma)
+                        REAL* caust, REAL* green, REAL* lepsi, REAL* seqvm, REAL* gp_sigma,
+                        REAL* gp_F, REAL* gp_P, REAL* gp_det, REAL* volum)
 {
+  if (volum) { volum[0] = 0; volum[1] = 0; }
   static const int vi[6] = {0, 1, 2, 1, 0, 0}, vj[6] = {0, 1, 2, 2, 2, 1};
   REAL posgp[24], weigp[8];
   FN(orc_hex8_gauss)(posgp, weigp);
@@ -922,6 +927,12 @@ int FN(orc_postprocess)(int nelem, int npoin, const int32_t* lnods, const REAL* 
       }
       if (gp_sigma)
         for (int v = 0; v < 6; ++v) gp_sigma[v + 6 * (g + 8 * (int64_t)e)] = M3(sig, vi[v], vj[v]);
+      for (int k = 0; k < 9; ++k) {
+        if (gp_F) gp_F[k + 9 * (g + 8 * (int64_t)e)] = F[k];
+        if (gp_P) gp_P[k + 9 * (g + 8 * (int64_t)e)] = P[k];
+      }
+      if (gp_det) gp_det[g + 8 * (int64_t)e] = detF;
+      if (volum) { volum[0] += volux; volum[1] += volux * detF; }
     }
   }
   for (int p = 0; p < npoin; ++p) {

@@ -186,6 +186,7 @@ def test_trajectory_fp64_matches_oracle(oracle, bar):
     assert abs(g.time - o.cutim[0]) <= 1e-18
     c = g.counters()
     assert c["nr_failed"] == 0 and c["nonfinite"] == 0 and c["neg_det"] == 0
+    assert c["gpdet_min"] == 0.0 and c["ielem_min"] == -1      # no det F <= 0 met
     assert c["nr_active"] > 0
 
 

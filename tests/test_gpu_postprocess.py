@@ -100,3 +100,44 @@ def test_postprocess_after_steps_is_repeatable():
     z = sma.ExplicitSolid(p, precision="fp64")
     r0 = z.postprocess()
     assert all(np.abs(r0[k]).max() == 0.0 for k in ("caust", "green", "lepsi", "seqvm"))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gauss_fields_match_oracle(oracle, precision):
+    """gpgdi, gppio, det F per Gauss point and volum_sld(1:2), from the same
+    evaluation as the stresses (the state the last element loop read)."""
+    p = P.cylinder_2m(nsteps=10, div=8)                         # per-element materials
+    g = sma.ExplicitSolid(p, precision=precision, scatter="color")
+    o = oracle.Problem(p)
+    u = _two_loops(g, o, p, (0.008, 0.02), 50.0)
+    got = g.gauss_fields()
+    ref = o.postprocess(u, slot=1, gauss=True)
+    tol = {"fp64": dict(gpgdi=1e-13, gppio=1e-8, gpdet=1e-13, volum=1e-12),
+           "fp32": dict(gpgdi=1e-6, gppio=1e-3, gpdet=1e-6, volum=1e-6)}[precision]
+    for k in ("gpgdi", "gppio", "gpdet", "volum"):
+        assert _rel(got[k], ref[k]) < tol[k], (k, _rel(got[k], ref[k]))
+    assert ref["volum"][1] > ref["volum"][0]                      # stretched: volume grew
+
+
+def test_negative_jacobian_report(oracle):
+    """An element turned inside out: the element loop counts the Gauss points
+    with det F <= 0 and reports the smallest det F and its element, as the
+    reference's gpdet_min / ielem_min (sld_elmpre.f90:229-238)."""
+    p = P.bar_40x4x4(nsteps=10, ref_equivalent=True)
+    u = np.zeros((p.npoin, 3))
+    q = int(np.argmin(np.sum((p.coord - [20.0, 2.0, 2.0]) ** 2, axis=1)))
+    u[q, 0] = 3.0                                                 # node pushed 3 element sizes along x
+    g = sma.ExplicitSolid(p, precision="fp64", scatter="color")
+    g.counters(reset=True)
+    g.assemble(u)
+    c = g.counters()
+    ref = oracle.Problem(p).assemble(u)
+    assert c["neg_det"] > 0
+    assert ref["gpdet_min"] < 0.0
+    assert abs(c["gpdet_min"] - ref["gpdet_min"]) <= 1e-6 * abs(ref["gpdet_min"])
+    assert q in p.lnods[c["ielem_min"]]                           # an element of the moved node
+    det = g.gauss_fields()["gpdet"]
+    assert abs(det[c["ielem_min"]].min() - det.min()) <= 1e-6 * abs(det.min())
+    g.counters(reset=True)
+    c = g.counters()
+    assert c["neg_det"] == 0 and c["ielem_min"] == -1
