@@ -207,8 +207,10 @@ def run_reference(args):
     base = cpu_baseline(prob, u0, budget_s=15.0, max_steps=max(2, args.steps))
     line = {"impl": "reference", "metric": "Gauss-point updates/s (explicit SMA step)",
             "value": base["value"], "unit": "GP-updates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": prob.nelem * 8 / base["value"] * 1e3, "higher_is_better": True,
+            "scaling": "strong" if (args.workload == "ensemble" and world > 1) else "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload], "nelem": prob.nelem, "npoin": prob.npoin,
                        "gauss_points": prob.nelem * 8, "precision": "fp64 (reference CPU path)",
                        "prestrain": args.prestrain},
