@@ -95,6 +95,8 @@ def lib():
         L.sma_assemble_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
         L.sma_end_step.argtypes = [C.c_void_p]
         L.sma_postprocess.argtypes = [C.c_void_p] * 6
+        L.sma_host_register.argtypes = [C.c_void_p, C.c_size_t]
+        L.sma_host_unregister.argtypes = [C.c_void_p]
         L.sma_gauss_fields.argtypes = [C.c_void_p] * 5
         L.sma_eval_law160.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
@@ -182,11 +184,17 @@ class ExplicitSolid:
         _check(lib().sma_explicit_step(self._ctx, int(nsteps)))
 
     # -- element-loop boundary ----------------------------------------------
-    def assemble(self, displ, fext_scale=0.0, want_all=True):
+    def assemble(self, displ, fext_scale=0.0, want_all=True, rhsid=None):
         """sld_matrix explicit: returns dict of (npoin,3) rhsid, finte, fexte,
-        frxid and (npoin,) vmass.  Reads state TIME_N, writes ITER_K."""
+        frxid and (npoin,) vmass.  Reads state TIME_N, writes ITER_K.  rhsid:
+        an optional caller-owned (npoin, 3) float64 output array (e.g. one
+        page-locked with host_register, like displ)."""
         d = np.ascontiguousarray(displ, dtype=np.float64).reshape(self.npoin, 3)
         out = {q: np.zeros((self.npoin, 3)) for q in ("rhsid", "finte", "fexte", "frxid")}
+        if rhsid is not None:
+            if rhsid.dtype != np.float64 or rhsid.shape != (self.npoin, 3) or not rhsid.flags["C_CONTIGUOUS"]:
+                raise ValueError("rhsid must be a C-contiguous float64 (npoin, 3) array")
+            out["rhsid"] = rhsid
         out["vmass"] = np.zeros(self.npoin)
         if not want_all:
             for q in ("finte", "fexte", "frxid", "vmass"):
@@ -327,6 +335,19 @@ class ExplicitSolid:
     @property
     def kernel_launches(self):
         return int(lib().sma_kernel_launches(self._ctx))
+
+
+def host_register(arr):
+    """Page-lock a C-contiguous numpy array in place (sma_host_register), so
+    ExplicitSolid.assemble's copies of it overlap the element loop."""
+    if not arr.flags["C_CONTIGUOUS"]:
+        raise ValueError("host_register needs a C-contiguous array")
+    _check(lib().sma_host_register(arr.ctypes.data, arr.nbytes))
+    return arr
+
+
+def host_unregister(arr):
+    _check(lib().sma_host_unregister(arr.ctypes.data))
 
 
 def eval_sld_stress_model_160(props, gpgdi, gpsdv, gptmp=None, flagt=0, e_mart=0.0,

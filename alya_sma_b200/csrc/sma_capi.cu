@@ -24,11 +24,16 @@ int32_t fail(int32_t code, const std::string& msg) {
   return code;
 }
 
+// A failing runtime call also leaves its error as the thread's "last error";
+// it is cleared here (non-sticky errors) so that a later launch check in
+// another entry point does not report it a second time.
 #define CU(call)                                                                   \
   do {                                                                             \
     cudaError_t e_ = (call);                                                       \
-    if (e_ != cudaSuccess)                                                         \
+    if (e_ != cudaSuccess) {                                                       \
+      cudaGetLastError();                                                          \
       return fail(SMA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    }                                                                              \
   } while (0)
 
 template <typename P>
@@ -814,6 +819,7 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   do {                                                                               \
     cudaError_t e_ = (call);                                                         \
     if (e_ != cudaSuccess) {                                                         \
+      cudaGetLastError();                                                            \
       sma_ctx_destroy(c);                                                            \
       return fail(SMA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     }                                                                                \
@@ -1092,6 +1098,18 @@ int32_t sma_assemble(sma_ctx* c, const double* displ, double fext_scale, double*
   }
   CU(cudaStreamSynchronize(c->stream));
   if (vmass) std::memcpy(vmass, c->vmass.data(), c->npoin * sizeof(double));
+  return SMA_OK;
+}
+
+int32_t sma_host_register(void* ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return fail(SMA_ERR_ARG, "NULL or empty host array");
+  CU(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return SMA_OK;
+}
+
+int32_t sma_host_unregister(void* ptr) {
+  if (!ptr) return fail(SMA_ERR_ARG, "NULL host array");
+  CU(cudaHostUnregister(ptr));
   return SMA_OK;
 }
 

@@ -23,6 +23,7 @@
 #ifndef ALYA_SMA_H
 #define ALYA_SMA_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -141,6 +142,12 @@ int32_t sma_explicit_step(sma_ctx* ctx, int32_t nsteps);
 int32_t sma_assemble(sma_ctx* ctx, const double* displ, double fext_scale,
                      double* rhsid, double* finte, double* fexte, double* frxid,
                      double* vmass);
+/* Page-lock a caller-owned host array (e.g. Alya's displ and rhsid) once, so
+ * sma_assemble's copies run asynchronously and overlap its element slabs;
+ * unregister before freeing the array.  No counterpart in the reference
+ * (its arrays never leave the host). */
+int32_t sma_host_register(void* ptr, size_t bytes);
+int32_t sma_host_unregister(void* ptr);
 /* same with device pointers (no host copies), ordered on the context stream */
 int32_t sma_assemble_device(sma_ctx* ctx, const double* d_displ, double fext_scale,
                             double* d_rhsid);
