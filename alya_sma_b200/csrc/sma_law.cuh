@@ -80,6 +80,15 @@ template <> struct Fm<double> {
          x2 * (1.0 / 355687428096000.0 + x2 * (-1.0 / 121645100408832000.0))))))))));
   }
   static __device__ __forceinline__ double clustered() { return 1e-8; }
+  // first divided difference f[u,v] of log1p, given fu = log1p(u), fv =
+  // log1p(v) and iv = 1/(1+v): the series of log1p(w)/w for near-equal
+  // arguments (|w| < 1e-3, w = (u-v)/(1+v)), else the difference quotient of
+  // the values already computed (cancellation below 1e-13 relative there)
+  static __device__ __forceinline__ double ddiff(double u, double v, double fu, double fv, double iv) {
+    const double w = (u - v) * iv;
+    if (fabs(w) < 1e-3) return log1p_ratio(w) * iv;
+    return (fu - fv) / (u - v);
+  }
 };
 
 template <> struct Fm<float> {
@@ -112,6 +121,11 @@ template <> struct Fm<float> {
          x2 * (-1.0f / 39916800))))));
   }
   static __device__ __forceinline__ float clustered() { return 1e-4f; }
+  // f[u,v] of log1p: the series of log1p(w)/w covers |w| <= 0.25, the
+  // strains of an explicit step (fu, fv unused)
+  static __device__ __forceinline__ float ddiff(float u, float v, float, float, float iv) {
+    return log1p_ratio((u - v) * iv) * iv;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -145,8 +159,8 @@ __device__ __forceinline__ void sym_log1p(const T* A, T* L, T* f) {
   const T fu = M::log1p_(u), fv = M::log1p_(v), fs = M::log1p_(s);
   f[0] = fs; f[1] = fu; f[2] = fv;
   const T iv = M::rcp(T(1) + v);
-  const T fuv = M::log1p_ratio((u - v) * iv) * iv;              // f[u,v]
-  const T fsv = M::log1p_ratio((s - v) * iv) * iv;              // f[s,v]
+  const T fuv = M::ddiff(u, v, fu, fv, iv);                     // f[u,v]
+  const T fsv = M::ddiff(s, v, fs, fv, iv);                     // f[s,v]
   const T dsu = s - u;
   T fsuv;                                                       // f[s,u,v]
   if (fabs(dsu) > M::clustered()) fsuv = M::div(fsv - fuv, dsu);
