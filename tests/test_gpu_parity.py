@@ -236,3 +236,26 @@ def test_precision_form_cantilever(oracle):
     rg, ro = g2.assemble(u), o2.assemble(u)
     rel_f = np.abs(rg["finte"] - ro["finte"]).max() / np.abs(ro["finte"]).max()
     assert rel_f < 1e-3, rel_f
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_patch_and_rigid_motion(bar, precision):
+    """Known answers of the element loop on the jittered bar, through the C
+    ABI: constant strain leaves no force on interior nodes; a finite rigid
+    rotation plus translation gives no force at all (FP32: the rounding of
+    F = R is a strain of ~1e-7)."""
+    import dataclasses
+    p = dataclasses.replace(bar, e_mart=np.full_like(bar.e_mart, bar.props[0, 0]))
+    X = p.coord
+    inner = np.all((X > X.min(axis=0) + 1e-9) & (X < X.max(axis=0) - 1e-9), axis=1)
+    rng = np.random.default_rng(3)
+    G = rng.normal(size=(3, 3)) * 1e-4
+    g = sma.ExplicitSolid(p, precision=precision)
+    r = g.assemble(X @ G.T, want_all=False)["rhsid"]
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    assert np.abs(r[inner]).max() <= tol * np.abs(r).max()
+    c, s = np.cos(0.7), np.sin(0.7)
+    R = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+    rr = g.assemble(X @ (R - np.eye(3)).T + np.array([3.0, -1.0, 2.0]), want_all=False)["rhsid"]
+    ref = g.assemble(X * np.array([1e-4, 0.0, 0.0]), want_all=False)["rhsid"]
+    assert np.abs(rr).max() <= (1e-9 if precision == "fp64" else 1e-2) * np.abs(ref).max()
