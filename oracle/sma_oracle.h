@@ -14,8 +14,10 @@
  * row's predecessor state (fixture tests/golden/data1_transitions.npz).  The
  * element loop, lumped mass and central-difference integrator have no
  * reference-computed golden output (the reference cannot be compiled without a
- * Fortran compiler); they are checked by analytic known answers (patch tests,
- * rigid motion, mass conservation, elastic wave speed).
+ * Fortran compiler); they are checked by analytic known answers: the constant-
+ * strain patch test on a jittered mesh, zero force under a finite rigid
+ * motion, lumped mass = rho V, and dt_crit = h / c on a regular mesh
+ * (tests/test_oracle_element.py).
  *
  * Every entry point exists twice: *_f64 (double, the oracle) and *_f32
  * (float, used only for precision studies of an all-FP32 CPU run).
