@@ -32,7 +32,7 @@ HEADER = os.path.join(os.path.dirname(PKG), "include", "alya_sma.h")
 PREC = {"fp64": 0, "fp32": 1}
 SCATTER = {"auto": 0, "atomic": 1, "color": 2}
 FIELD = {"displ": 0, "veloc": 1, "accel": 2, "rhsid": 3, "vmass": 4}
-COUNTERS = ["nr_active", "nr_failed", "nr_both", "neg_det", "nonfinite", "fallback64"]
+COUNTERS = ["nr_active", "nr_failed", "nr_both", "neg_det", "nonfinite"]
 
 
 class SmaError(RuntimeError):

@@ -24,7 +24,7 @@ constexpr int MAXFUN = 16;
 constexpr int MAXPTS = 32;
 
 enum Cnt { CNT_NR_ACTIVE = 0, CNT_NR_FAILED, CNT_NR_BOTH, CNT_NEG_DET, CNT_NONFINITE,
-           CNT_FALLBACK64, CNT_DETMIN, NCNT = 8 };
+           CNT_RESERVED5, CNT_DETMIN, NCNT = 8 };
 
 // CNT_DETMIN holds min over Gauss points with det F <= 0 of (det F, element)
 // packed for one 64-bit atomicMin: the float's bits mapped to an unsigned

@@ -62,7 +62,7 @@ extern "C" {
 #define SMA_CNT_NR_BOTH     2   /* AS and SA active together                    */
 #define SMA_CNT_NEG_DET     3   /* Gauss points with det F <= 0                 */
 #define SMA_CNT_NONFINITE   4   /* non-finite nodal accelerations               */
-#define SMA_CNT_FALLBACK64  5   /* FP32 points re-evaluated by the FP64 law     */
+                            /* 5..7: reserved, read as 0                     */
 #define SMA_NCOUNTERS       8
 
 typedef struct sma_ctx sma_ctx;
