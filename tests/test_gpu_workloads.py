@@ -1,6 +1,6 @@
-"""Workload paths of the north-star configurations at oracle-sized
-resolution: per-element materials and a temperature field (the O-grid
-cylinder), the batched ensemble, and the autotuner."""
+"""The cylinder and ensemble workloads at oracle-sized resolution:
+per-element materials and a temperature field (the O-grid cylinder), the
+batched ensemble, and the autotuner."""
 import numpy as np
 import pytest
 
