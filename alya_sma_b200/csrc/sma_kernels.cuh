@@ -282,8 +282,8 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
     q[6 + m] = t02 * B[3 * m + 0] + t12 * B[3 * m + 1] + t22 * B[3 * m + 2];
   }
   // body force of the Gauss point, dV rho (g - alpha v(g)): gravity
-  // (elfext) and the Rayleigh alpha term (elrayl_alpha, sld_elmmat.f90:156-
-  // 159) with v(g) = sum_b N_b(g) v_b from the element's lanes by shuffle
+  // (elfext) and the Rayleigh alpha term (elrayl_alpha, sld_elmmat.f90:159-
+  // 164) with v(g) = sum_b N_b(g) v_b from the element's lanes by shuffle
   const bool body = DAMP || a.has_grav;
   if (body) {
     const T rho = (T)mat.densi;
@@ -564,8 +564,8 @@ inline size_t element_pipe_smem_bytes(int block, bool mats) {
 }
 
 // ---------------------------------------------------------------------------
-// Stress/strain post-processing (sld_calculate_pp_tensors_ielem.f90:100-150,
-// 180-218; itask 3 of the element loop).  Lane = Gauss point: the law is
+// Stress/strain post-processing (sld_calculate_pp_tensors_ielem.f90:110-150,
+// 186-218; itask 3 of the element loop).  Lane = Gauss point: the law is
 // evaluated from the state in a.sold (its new state is discarded), then
 //   sigma = tau / det F                  (= F P^T / det F of the reference)
 //   E     = (H + H^T + H^T H) / 2        (Green strain, = (F^T F - I) / 2)
@@ -821,7 +821,7 @@ __global__ void __launch_bounds__(256) k_nodal(NodalArgs a) {
         if (ENERGY) {                                     // mod_sld_energy.f90:71-193
           const double uk = a.u[k];
           const double fx = (fl & 8u) ? a.fext[k] * ts.load : 0.0;
-          // r = fext - fint - f_rayleigh (sld_elmmat.f90:168)
+          // r = fext - fint - f_rayleigh (sld_elmmat.f90:170)
           const double fi = fx - r - (a.fray ? a.fray[k] : 0.0);
           const double dd = uk - a.uprev[k];
           e_ie += (fi + a.fint_prev[k]) * dd;
@@ -1002,7 +1002,7 @@ __global__ void k_outputs(const double* f, const double* fext, const uint8_t* fl
 }
 
 // The Rayleigh alpha nodal force alone, sum_e sum_g N_a(g) dV rho alpha v(g)
-// (elrayl_alpha of sld_elmmat.f90:156-159), FP64, one thread per element,
+// (elrayl_alpha of sld_elmmat.f90:159-164), FP64, one thread per element,
 // added into fray (SoA [3][npad], zeroed by the caller).  The element kernel
 // already folds this force into the residual; this pass exists so that the
 // internal force of the energy balance and of sma_assemble's finte leaves it

@@ -82,7 +82,7 @@ typedef struct {
   const double* tempe;      /* (nelem) temperature (extension) or NULL         */
   const double* dampi;      /* (2, nmate) Rayleigh (alpha, beta) or NULL:       */
                             /* RAYLEIGH_DAMPING of sld_reaphy.f90:1048-1055;    */
-                            /* alpha (mass-proportional, sld_elmmat.f90:156-159) */
+                            /* alpha (mass-proportional, sld_elmmat.f90:159-164) */
                             /* is applied; beta > 0 is rejected (SMA_ERR_ARG)   */
 } sma_material_desc;
 
@@ -165,7 +165,7 @@ int32_t sma_end_step(sma_ctx* ctx);
  * sma_assemble it reproduces that loop's stresses; the state is not changed.
  * Replaces sld_calculate_pp_tensors (sld_calculate_pp_tensors.f90:40-145)
  * with sld_calculate_pp_tensors_ielem (sld_calculate_pp_tensors_ielem.f90:
- * 100-150 and 180-218, itask 3 of sld_elmope). */
+ * 110-150 and 186-218, itask 3 of sld_elmope). */
 int32_t sma_postprocess(sma_ctx* ctx, double* caust, double* green, double* lepsi,
                         double* seqvm, double* gp_sigma);
 

@@ -553,7 +553,7 @@ int FN(orc_element)(const REAL elcod[24], const REAL eldis[24], const REAL props
 
     /* internal/external forces, sld_elmmat.f90:137-166 (no prestress), and
      * the Rayleigh alpha force alpha v(g) N_a rho dV with the Gauss-point
-     * velocity v(g) = sum_b N_b elvel_b (sld_elmpre.f90:114, :160-163) */
+     * velocity v(g) = sum_b N_b elvel_b (sld_elmpre.f90:114), sld_elmmat.f90:159-164 */
     REAL gpvel[3] = {0, 0, 0};
     if (elvel && ray_alpha > 0)
       for (int i = 0; i < 3; ++i)
@@ -583,7 +583,7 @@ int FN(orc_element)(const REAL elcod[24], const REAL eldis[24], const REAL props
  * coefficients (alpha, beta) of sld_reaphy.f90:1048-1055 (NULL: none); the
  * alpha force uses the nodal velocity veloc (the ITER_K velocity the element
  * loop gathers, sld_elmgat.f90:60) and enters rhsid and frxid only, not
- * finte or fexte (sld_elmmat.f90:168).  beta is not restated (see
+ * finte or fexte (sld_elmmat.f90:170).  beta is not restated (see
  * orc_run_cd). */
 int FN(orc_assemble)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
                      const REAL* displ, const int32_t* lmate, const REAL* props,
@@ -637,7 +637,7 @@ int FN(orc_assemble)(int nelem, int npoin, const int32_t* lnods, const REAL* coo
         for (int a = 0; a < 8; ++a) {
           int64_t p = ln[a];
           for (int i = 0; i < 3; ++i) {
-            /* elrhs = elfext - elfint - elrayl_alpha, sld_elmmat.f90:168 */
+            /* elrhs = elfext - elfint - elrayl_alpha, sld_elmmat.f90:170 */
             REAL elrhs = elfext[i + 3 * a] - elfint[i + 3 * a] - elrayl[i + 3 * a];
             rhsid[i + 3 * p] += elrhs;
             if (finte) finte[i + 3 * p] += elfint[i + 3 * a];
@@ -729,8 +729,8 @@ REAL FN(orc_critical_dt)(int nelem, const int32_t* lnods, const REAL* coord,
  * dampi (2, nmate, NULL: none): Rayleigh alpha damping with the velocity the
  * reference holds in veloc(ITER_K) during the element loop -- the step-
  * boundary velocity v_n in the central-difference scheme (written by the
- * previous corrector, :201), the predicted v_n + dt a_n in Tchamwa-Wielgosz
- * (:413).  The stiffness-proportional beta term (sld_elmmat.f90:170-190) is
+ * previous corrector, :202), the predicted v_n + dt a_n in Tchamwa-Wielgosz
+ * (:413).  The stiffness-proportional beta term (sld_elmmat.f90:172-190) is
  * not restated: no reference deck sets RAYBETA and its term is marked for
  * revision there; the CUDA library rejects beta > 0. */
 int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord,
@@ -819,8 +819,8 @@ int FN(orc_run_cd)(int nelem, int npoin, const int32_t* lnods, const REAL* coord
 
 /* ------------------------------------------------------------------------ */
 /* Stress and strain post-processing: sld_calculate_pp_tensors.f90:40-145    */
-/* with sld_calculate_pp_tensors_ielem.f90:100-150 (itask 3: Cauchy stress,  */
-/* Green strain) and :180-218 (logarithmic strain).  Per Gauss point          */
+/* with sld_calculate_pp_tensors_ielem.f90:110-150 (itask 3: Cauchy stress,  */
+/* Green strain) and :186-218 (logarithmic strain).  Per Gauss point          */
 /*   sigma(i,j) = sum_k F(i,k) P(j,k) / det F                                 */
 /*   E(i,j)     = sum_k F(k,i) F(k,j) / 2 - delta_ij / 2                      */
 /*   lnV(i,j)   = sum_k log(sqrt(|w_k|)) n_k(i) n_k(j),  (w, n) eig(F F^T)     */

@@ -53,7 +53,7 @@ def test_tw_scheme_matches_oracle(oracle, bar):
 @pytest.mark.parametrize("scheme", ["cd", "tw"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_rayleigh_alpha_damping_matches_oracle(oracle, bar, scheme, precision):
-    """RAYLEIGH_DAMPING RAYALPHA (sld_elmmat.f90:156-159): the element loop
+    """RAYLEIGH_DAMPING RAYALPHA (sld_elmmat.f90:159-164): the element loop
     subtracts alpha rho N v(g) dV with the velocity the reference's loop reads
     (v_n in central differences, the predicted velocity in TW)."""
     import dataclasses
@@ -78,7 +78,7 @@ def test_rayleigh_alpha_damping_matches_oracle(oracle, bar, scheme, precision):
 
 def test_rayleigh_assemble_keeps_damping_out_of_finte(oracle, bar):
     """sma_assemble with damping: rhsid and frxid carry the Rayleigh force,
-    finte and fexte do not (sld_elmmat.f90:168, sld_element_operations)."""
+    finte and fexte do not (sld_elmmat.f90:170, sld_element_operations)."""
     import dataclasses
     p = dataclasses.replace(bar, dampi=np.array([[3.0e5, 0.0]]))
     rng = np.random.default_rng(7)
