@@ -83,6 +83,25 @@ def test_pipelined_assemble_equals_serial(canti):
     _compare(canti, u, canti, u)
 
 
+def test_pipelined_assemble_with_damping(canti):
+    """Rayleigh alpha damping through the pipelined boundary (the one-tile
+    damped kernel per slab, the velocity as set) equals the serial path."""
+    p = dataclasses.replace(canti, dampi=np.array([[2.0e5, 0.0]]))
+    u = _field(p, 0)
+    v = np.random.default_rng(5).normal(size=(p.npoin, 3)) * 1e3
+    out = []
+    for scatter in ("atomic", "color"):
+        g = sma.ExplicitSolid(p, precision="fp64", scatter=scatter)
+        g.set("veloc", v)
+        out.append(g.assemble(u, fext_scale=0.5))
+    und = sma.ExplicitSolid(canti, precision="fp64").assemble(u, fext_scale=0.5)
+    for k in ("rhsid", "finte", "frxid"):
+        scale = max(np.abs(out[1][k]).max(), 1e-30)
+        assert np.abs(out[0][k] - out[1][k]).max() <= 1e-11 * scale, k
+    assert np.abs(out[0]["finte"] - und["finte"]).max() <= 1e-11 * np.abs(und["finte"]).max()
+    assert np.abs(out[0]["rhsid"] - und["rhsid"]).max() > 1e-3 * np.abs(und["rhsid"]).max()
+
+
 def test_registered_host_arrays(canti):
     """Page-locked caller arrays (sma_host_register) give the same residual as
     pageable ones, and unregister cleanly."""
