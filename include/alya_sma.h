@@ -106,7 +106,7 @@ typedef struct {
 } sma_run_desc;
 
 /* element-loop kernels */
-#define SMA_VARIANT_AUTO    0   /* FP32: PIPE, FP64: PLAIN (measured on B200)                 */
+#define SMA_VARIANT_AUTO    0   /* PLAIN in both precisions (measured on B200)                */
 #define SMA_VARIANT_PIPE    1   /* persistent blocks, next tile's gather in flight (cp.async) */
 #define SMA_VARIANT_PLAIN   2   /* one tile per block                                        */
 
