@@ -105,17 +105,17 @@ def _funbou(oracle, tab, smooth, t):
     return fn(tb.shape[0], tb.ctypes.data_as(C.POINTER(C.c_double)), int(smooth), 0, float(t))
 
 
-@pytest.mark.parametrize("alpha", [0.0, 1.0e5])
-def test_energy_balance_matches_restatement(oracle, canti, alpha):
+@pytest.mark.parametrize("alpha,scheme", [(0.0, "cd"), (1.0e5, "cd"), (0.0, "tw")])
+def test_energy_balance_matches_restatement(oracle, canti, alpha, scheme):
     """ALLIE/ALLWK/ALLKE/ETOTA/EENER of mod_sld_energy.f90:71-193, computed by
     the device after every step, against the same formulas evaluated on
-    oracle step snapshots.  With Rayleigh damping the internal force of the
-    balance is finte, which leaves the damping force out as the reference's
-    does."""
+    oracle step snapshots (central difference and Tchamwa-Wielgosz).  With
+    Rayleigh damping the internal force of the balance is finte, which leaves
+    the damping force out as the reference's does."""
     import dataclasses
     p = dataclasses.replace(canti, dampi=np.array([[alpha, 0.0]])) if alpha else canti
     nsteps = 200
-    g = sma.ExplicitSolid(p, precision="fp64")
+    g = sma.ExplicitSolid(p, precision="fp64", scheme=scheme)
     g.set_energy(True, nsteps)
     g.step(nsteps)
     tot, hist = g.energy()
@@ -132,7 +132,7 @@ def test_energy_balance_matches_restatement(oracle, canti, alpha):
     for s in range(nsteps):
         u0 = o.displ.copy()
         v0, sdv0 = o.veloc.copy(), o.sdv.copy()
-        o.run(p.dtime, 1)
+        o.run(p.dtime, 1, scheme=scheme, phi=1.033)
         fx = p.fext * _funbou(oracle, tab, p.fun_smooth[p.load_fun], o.cutim[0])
         if alpha:
             side.sdv[:] = sdv0
