@@ -259,3 +259,31 @@ def test_patch_and_rigid_motion(bar, precision):
     rr = g.assemble(X @ (R - np.eye(3)).T + np.array([3.0, -1.0, 2.0]), want_all=False)["rhsid"]
     ref = g.assemble(X * np.array([1e-4, 0.0, 0.0]), want_all=False)["rhsid"]
     assert np.abs(rr).max() <= (1e-9 if precision == "fp64" else 1e-2) * np.abs(ref).max()
+
+
+def test_full_load_cycle_within_the_laws_own_sensitivity(oracle):
+    """The whole 40x4x4 bar load cycle (4,000 steps: pull to 6 % strain and
+    release).  During loading the GPU and the oracle agree to round-off; in
+    the reverse transformation the law's strict activation inequalities
+    (sld_stress_model_160.f90:351,368) amplify round-off by ~1e9, so over the
+    full cycle the GPU is held to the oracle's own sensitivity: the oracle
+    against itself with coordinates scaled by (1 + 1e-15)."""
+    import dataclasses
+    p = P.bar_40x4x4(nsteps=4000)
+    mid = int(np.argmin(np.sum((p.coord - [20, 2, 2]) ** 2, axis=1)))
+    q = int(np.argmin(np.sum((p.coord - [30, 4, 0]) ** 2, axis=1)))
+    wit = [3 * mid, 3 * mid + 1, 3 * q, 3 * q + 2]
+    h_ref = oracle.Problem(p).run(p.dtime, 4000, wit_dof=wit)
+    pert = dataclasses.replace(p, coord=p.coord * (1 + 1e-15))
+    h_self = oracle.Problem(pert).run(p.dtime, 4000, wit_dof=wit)
+    scale = np.abs(h_ref).max()
+    e_self = np.abs(h_self - h_ref).max(axis=1) / scale
+    out = {}
+    for prec in ("fp64", "fp32"):
+        g = sma.ExplicitSolid(p, precision=prec, scatter="color")
+        g.set_witness(wit, 4000)
+        g.step(4000)
+        out[prec] = np.abs(g.witness() - h_ref).max(axis=1) / scale
+    assert out["fp64"][:3000].max() < 1e-9                        # loading and plateau: round-off
+    assert out["fp64"].max() <= 10 * e_self.max() + 1e-9           # whole cycle: the law's own spread
+    assert out["fp32"][:2000].max() < 1e-4                         # precision form, loading half
