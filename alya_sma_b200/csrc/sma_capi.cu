@@ -300,6 +300,9 @@ namespace {
 // maxima; a device that refuses it (MIG, older parts) just runs without.
 void set_l2_window(sma_ctx* c, void* base, size_t bytes, const cudaDeviceProp& prop) {
   if (prop.persistingL2CacheMaxSize <= 0 || prop.accessPolicyMaxWindowSize <= 0) return;
+  // only when the arrays fit the carve-out whole: a larger window (2.0 M-element
+  // cylinder, 146 MB) thrashed it and made both kernels ~2x slower on B200
+  if (bytes > (size_t)prop.persistingL2CacheMaxSize || bytes > (size_t)prop.accessPolicyMaxWindowSize) return;
   const size_t win = std::min<size_t>(bytes, (size_t)prop.accessPolicyMaxWindowSize);
   size_t lim = std::min<size_t>(win, (size_t)prop.persistingL2CacheMaxSize);
   size_t cur = 0;

@@ -280,15 +280,25 @@ def critical_dt(coord, lnods, props, densi, lmate=None):
 
 
 def prestrain(prob, eps, nu_eff=0.45):
-    """Displacement field of a uniform axial strain eps along x with lateral
-    contraction nu_eff about the cross-section centre, zero on prescribed
-    dofs.  Used to start a timed run on the transformation plateau, where
-    every Gauss point runs the full return map."""
+    """Axial prestrain along x with lateral contraction nu_eff about the
+    cross-section centre, compatible with the prescribed dofs (their tables
+    start at 0): a uniform strain eps when the x = max end is free, and
+    u_x = eps L s (1 - s), s = (x - x_min) / L, when that end is held too
+    (strain from +eps to -eps, zero displacement at both ends; a uniform
+    field there would crush the last element layer).  Used to start a timed
+    run on the transformation plateau, where Gauss points run the return map."""
     X = prob.coord
+    x0, L = X[:, 0].min(), X[:, 0].max() - X[:, 0].min()
+    s = (X[:, 0] - x0) / L
     yc = 0.5 * (X[:, 1].min() + X[:, 1].max())
     zc = 0.5 * (X[:, 2].min() + X[:, 2].max())
-    u = np.stack([eps * (X[:, 0] - X[:, 0].min()), -nu_eff * eps * (X[:, 1] - yc),
-                  -nu_eff * eps * (X[:, 2] - zc)], axis=1)
+    far = np.isclose(s, 1.0)
+    held = bool(np.any(prob.fixno[far, 0] == 1))
+    if held:
+        ux, ex = eps * L * s * (1.0 - s), eps * (1.0 - 2.0 * s)
+    else:
+        ux, ex = eps * L * s, np.full_like(s, eps)
+    u = np.stack([ux, -nu_eff * ex * (X[:, 1] - yc), -nu_eff * ex * (X[:, 2] - zc)], axis=1)
     u[prob.fixno == 1] = 0.0
     return u
 
