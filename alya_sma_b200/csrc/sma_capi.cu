@@ -367,9 +367,12 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance, bool stepping 
 template <typename T>
 using ElemKernel = void (*)(ElemArgs<T>);
 
+// one-tile kernels: the narrow instance (tighter register cap, more warps)
+// for blocks of up to ELEM_NARROW_BLOCK threads, the wide one above
 template <typename T, bool ATOMIC, bool MATS>
-ElemKernel<T> elem_kernel_v(bool pipe) {
-  return pipe ? k_element_pipe<T, ATOMIC, MATS> : k_element<T, ATOMIC, MATS>;
+ElemKernel<T> elem_kernel_v(bool pipe, int block) {
+  if (pipe) return k_element_pipe<T, ATOMIC, MATS>;
+  return block <= ELEM_NARROW_BLOCK ? k_element<T, ATOMIC, MATS, false, true> : k_element<T, ATOMIC, MATS>;
 }
 
 template <typename T>
@@ -377,12 +380,13 @@ ElemKernel<T> elem_kernel(const sma_ctx* c) {
   const bool pipe = c->variant == SMA_VARIANT_PIPE;
   const bool atomic = c->scatter != SMA_SCATTER_COLOR;
   const bool mats = c->d_lmate != nullptr;
+  const int b = c->block;
   if (c->damp) {                                                 // one-tile kernel only
     if (atomic) return mats ? k_element<T, true, true, true> : k_element<T, true, false, true>;
     return mats ? k_element<T, false, true, true> : k_element<T, false, false, true>;
   }
-  if (atomic) return mats ? elem_kernel_v<T, true, true>(pipe) : elem_kernel_v<T, true, false>(pipe);
-  return mats ? elem_kernel_v<T, false, true>(pipe) : elem_kernel_v<T, false, false>(pipe);
+  if (atomic) return mats ? elem_kernel_v<T, true, true>(pipe, b) : elem_kernel_v<T, true, false>(pipe, b);
+  return mats ? elem_kernel_v<T, false, true>(pipe, b) : elem_kernel_v<T, false, false>(pipe, b);
 }
 
 template <typename T>

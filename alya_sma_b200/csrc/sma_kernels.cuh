@@ -364,21 +364,35 @@ __device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC
   else return a.mat0;
 }
 
-// Minimum resident blocks of 256 threads the element kernels are compiled
-// for, which caps their registers at 65536 / (256 x blocks).  Measured on
-// B200 over fixed step windows: the one-tile FP32 kernel with one material is
-// fastest at 3 (80 registers, 24 warps per SM, 20 bytes of spills); with
-// per-element materials, in the pipelined kernel and in FP64 the spills of
-// a tighter cap cost more than the extra warps gain, so 2 (128 registers).
-template <typename T, bool PIPE, bool MATS>
-constexpr int elem_min_blocks() { return (sizeof(T) == 4 && !PIPE && !MATS) ? 3 : 2; }
+// Launch bounds of the element kernels: the largest block (NARROW: 128
+// threads, the one-tile default; else 256) and the minimum resident blocks,
+// which cap registers at 65536 / (threads x blocks).  Measured on B200 over
+// fixed step windows of the one-tile kernel:
+//   FP32, one material: 80 registers at either width (6 x 128 or 3 x 256,
+//     24 warps per SM, no spills);
+//   FP32 with per-element materials, and FP64: 96 registers at 5 x 128 (20
+//     warps, 24-120 bytes of spills) beat 128 registers at 16 warps by 2-8%
+//     (FP64 cantilever 0.399 -> 0.367 ms, FP32 ensemble 1.643 -> 1.611 ms);
+//     80 registers at 24 warps lost 10% on the ensemble, 168 registers at 12
+//     warps lost 17% on the FP64 cantilever;
+//   256-thread blocks with per-element materials or FP64, and the pipelined
+//     kernel: 2 x 256 (128 registers).
+template <typename T, bool PIPE, bool MATS, bool NARROW = false>
+constexpr int elem_min_blocks() {
+  if (PIPE) return 2;
+  if (NARROW) return (sizeof(T) == 4 && !MATS) ? 6 : 5;
+  return (sizeof(T) == 4 && !MATS) ? 3 : 2;
+}
+constexpr int ELEM_NARROW_BLOCK = 128;
 
 // One tile of elements per block: each lane gathers its node with __ldg,
 // takes node 1's values from lane 0 of its element by shuffle.  MATS: the
 // mesh has per-element materials (lmate), copied into shared memory per
-// element.  DAMP: Rayleigh alpha damping with the velocity a.vel.
-template <typename T, bool ATOMIC, bool MATS, bool DAMP = false>
-__global__ void __launch_bounds__(256, (elem_min_blocks<T, false, MATS>())) k_element(ElemArgs<T> a) {
+// element.  DAMP: Rayleigh alpha damping with the velocity a.vel.  NARROW:
+// compiled for blocks of at most ELEM_NARROW_BLOCK threads.
+template <typename T, bool ATOMIC, bool MATS, bool DAMP = false, bool NARROW = false>
+__global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
+                                  (elem_min_blocks<T, false, MATS, NARROW>())) k_element(ElemArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tab = reinterpret_cast<T*>(smem_raw);                       // [8][8][4]
   T* elem_sm = tab + 256;

@@ -129,10 +129,20 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(precision):
-    """DRAM bytes per element-kernel launch from the committed ncu summary
-    (profiles/k_element_<precision>_cantilever.md, line 'dram_bytes_per_launch: N')."""
-    path = os.path.join(ROOT, "profiles", f"k_element_{precision}_cantilever.md")
+def profile_summary(precision, workload, div):
+    """The committed ncu summary of the element kernel on this exact workload
+    (profiles/k_element_<precision>_<workload>.md), or None: a figure taken on
+    one mesh says nothing about a launch on another."""
+    if div != 1:
+        return None
+    return os.path.join(ROOT, "profiles", f"k_element_{precision}_{workload}.md")
+
+
+def profiled_traffic(path):
+    """DRAM bytes per element-kernel launch from an ncu summary
+    (line 'dram_bytes_per_launch: N')."""
+    if path is None:
+        return None
     try:
         m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
         return float(m.group(1)) if m else None
@@ -140,10 +150,11 @@ def profiled_traffic(precision):
         return None
 
 
-def profiled_issue(precision):
+def profiled_issue(path):
     """Warp instructions per element-kernel launch from the same ncu summary
     (line 'warp_inst_per_launch: N'); the B200 has 148 SMs."""
-    path = os.path.join(ROOT, "profiles", f"k_element_{precision}_cantilever.md")
+    if path is None:
+        return None
     try:
         m = re.search(r"warp_inst_per_launch:\s*([0-9.eE+]+)", open(path).read())
         return {"warp_inst": float(m.group(1)), "sms": 148} if m else None
@@ -302,7 +313,8 @@ def main():
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes(prob, args.precision)
     achieved = alg / (el_ms / 1e3) / 1e9
-    traffic = profiled_traffic(args.precision)
+    summary = profile_summary(args.precision, args.workload, args.div)
+    traffic = profiled_traffic(summary)
     roofline = {"bound": "hbm", "kernel": "k_element", "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -311,7 +323,7 @@ def main():
                 "window": "the K timed steps replayed from a checkpoint of their start, "
                           "CUDA events around each launch on the library stream",
                 "note": "compute-bound kernel: the FP32/FP64 pipes, not HBM, bind it"}
-    issue = profiled_issue(args.precision)
+    issue = profiled_issue(summary)
     if issue:
         # instruction-issue roofline: warp instructions per launch (ncu) over
         # the measured launch time, against 4 issue slots per SM per clock

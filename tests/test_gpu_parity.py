@@ -152,6 +152,42 @@ def test_element_loop_matches_oracle(oracle, bar, precision, scatter, tol):
     g.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("mesh", ["bar", "cylinder"])
+def test_every_block_width_matches_oracle(oracle, bar, mesh, precision):
+    """The element kernel is compiled twice: for blocks of at most 128 threads
+    (a tighter register cap, more warps per SM) and for up to 256.  Both,
+    with one material and with per-element materials, give the oracle's
+    residual and state; the two colour-scatter FP64 results agree to
+    round-off."""
+    if mesh == "bar":
+        p, u = bar, deformed(bar, seed=3, strain=0.03)
+    else:
+        p = P.cylinder_2m(nsteps=600, div=8)
+        u = P.prestrain(p, 0.03) + np.random.default_rng(3).normal(size=p.coord.shape) * 1e-4
+        u[p.fixno == 1] = 0.0
+    o = oracle.Problem(p)
+    ro = o.assemble(u)
+    o.end_step()
+    so = o.sdv[:, 1, :, 0]
+    assert so.max() > 0.0                                  # martensite forms
+    scale = np.abs(ro["finte"]).max()
+    tol, tol_x = (1e-8, 1e-8) if precision == "fp64" else (1e-3, 2e-3)
+    rhs = {}
+    for block in (64, 128, 192, 256):
+        g = sma.ExplicitSolid(p, precision=precision, scatter="color", block=block)
+        rg = g.assemble(u)
+        g.end_step()
+        for q in ("rhsid", "finte"):
+            err = np.abs(rg[q] - ro[q]).max() / scale
+            assert err < tol, (block, q, err)
+        assert np.abs(g.state[:, 1, :, 0] - so).max() < tol_x, block
+        rhs[block] = rg["rhsid"]
+        g.close()
+    if precision == "fp64":
+        assert np.abs(rhs[128] - rhs[256]).max() <= 1e-12 * scale
+
+
 def test_colour_scatter_is_deterministic(bar):
     runs = []
     for _ in range(2):
