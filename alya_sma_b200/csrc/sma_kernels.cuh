@@ -192,43 +192,62 @@ __device__ __forceinline__ void lds8(const double* p, double* v) {
   }
 }
 
-// Phase 1 of a tile, lane = Gauss point g: J = dX/dxi and Gu = du/dxi from
-// the element's node rows in shared memory (relative to node 1, so node 1
-// drops out), Ji = J^-1 (Ji[3j+k] = dxi_j/dX_k) and H = dU/dX = Gu Ji
-// (jacobi.f90:172-219, sld_elmpre.f90:149-162).  Returns det J.
+// The element's node rows in shared memory, [6][8] (x, y, z, ux, uy, uz of
+// its 8 nodes relative to node 1), as their Walsh-Hadamard transform across
+// the element's 8 lanes: lane k stores W_k = sum_a v_a (-1)^popc(a & k).
+// A trilinear field sum_a v_a N_a(s,t,z) has, with the brick's node signs
+// (s = +1 where bit0 ^ bit1 of a, t = +1 where bit1, z = +1 where bit2,
+// mod_lagrange.f90:935-977),
+//   8 d/ds = -W3 + W1 t + W7 z - W5 t z
+//   8 d/dt = -W2 + W1 s + W6 z - W5 s z
+//   8 d/dz = -W4 + W7 s + W6 t - W5 s t,
+// so a Gauss point's 18 derivatives take 54 FMAs instead of 126, after three
+// shuffle butterfly stages shared by the element's lanes.
 template <typename T>
-__device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H, T* Jc = nullptr) {
-  T J[9], Gu[9];
-  {
-    // this lane's Gauss point: derivatives in registers (a table row per
-    // lane would put the 8 lanes of an element in one shared-memory bank)
-    T N[8], dN[24];
-    hex8_gp<T>(g, N, dN);
+__device__ __forceinline__ void stage_node_rows(T* nsm, int lane8, const T* v) {
+  T w[6];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) { J[k] = T(0); Gu[k] = T(0); }
+  for (int c = 0; c < 6; ++c) w[c] = v[c];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      T v[8];
-      lds8(nsm + 8 * c, v);
+  for (int m = 1; m < 8; m <<= 1) {
+    const T sg = (lane8 & m) ? T(-1) : T(1);                     // low lane w + p, high lane p - w
 #pragma unroll
-      for (int n = 1; n < 8; ++n) {
-        T* acc = (c < 3) ? J + 3 * c : Gu + 3 * (c - 3);
-        acc[0] += v[n] * dN[3 * n + 0];
-        acc[1] += v[n] * dN[3 * n + 1];
-        acc[2] += v[n] * dN[3 * n + 2];
-      }
-    }
+    for (int c = 0; c < 6; ++c) w[c] = fma(sg, w[c], __shfl_xor_sync(0xffffffffu, w[c], m));
   }
-  const T detJ = inv3(J, Ji);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) nsm[8 * c + lane8] = w[c];
+}
+
+// Phase 1 of a tile, lane = Gauss point g (s, t, z from bits 2, 1, 0 of g,
+// as hex8_gp): J8 = 8 dX/dxi and Gu8 = 8 du/dxi from the transformed node
+// rows (stage_node_rows), Ji = J8^-1 and H = dU/dX = Gu8 J8^-1 (jacobi.f90:
+// 172-219, sld_elmpre.f90:149-162), Jc8 = 8 F J = J8 + Gu8 if asked.
+// Returns det J.
+template <typename T>
+__device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H, T* Jc8 = nullptr) {
+  const T p = T(0.577350269189626);
+  const T s = (g & 4) ? p : -p, t = (g & 2) ? p : -p, z = (g & 1) ? p : -p;
+  const T st = s * t, tz = t * z, sz = s * z;
+  T J[9], Gu[9];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    T w[8];
+    lds8(nsm + 8 * c, w);
+    T* d = (c < 3) ? J + 3 * c : Gu + 3 * (c - 3);
+    d[0] = w[1] * t + w[7] * z - w[5] * tz - w[3];
+    d[1] = w[1] * s + w[6] * z - w[5] * sz - w[2];
+    d[2] = w[7] * s + w[6] * t - w[5] * st - w[4];
+  }
+  const T det8 = inv3(J, Ji);                                    // det(8 J) = 512 det J
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       H[3 * i + k] = Gu[3 * i + 0] * Ji[0 + k] + Gu[3 * i + 1] * Ji[3 + k] + Gu[3 * i + 2] * Ji[6 + k];
-  if (Jc)                                                        // F J = dx/dxi = J + Gu
+  if (Jc8)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Jc[k] = J[k] + Gu[k];
-  return detJ;
+    for (int k = 0; k < 9; ++k) Jc8[k] = J[k] + Gu[k];
+  return det8 * T(1.0 / 512.0);
 }
 
 // Work of one lane (element le, lane a) on one tile once its node is
@@ -247,16 +266,15 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
                                              const double* dX, const double* dU,
                                              double xS, double F_AS, double F_SA,
                                              const MatC& mat, double tmp, const T* Vn) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    nsm[8 * c + lane8] = (T)dX[c];
-    nsm[8 * (3 + c) + lane8] = (T)dU[c];
+  {
+    const T v[6] = {(T)dX[0], (T)dX[1], (T)dX[2], (T)dU[0], (T)dU[1], (T)dU[2]};
+    stage_node_rows<T>(nsm, lane8, v);
   }
   const int64_t gp = 8 * ec + lane8;
   __syncwarp();                                                  // node rows of the element
 
   // ---- phase 1, lane = Gauss point g ------------------------------------
-  T Ji[9], H[9], Jc[9];                                          // Jc = F J, live across the law
+  T Ji[9], H[9], Jc[9];                                          // Jc = 8 F J, live across the law
   const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H, Jc);
 
   // ---- constitutive update ----------------------------------------------
@@ -269,11 +287,12 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   }
 
   // ---- force operator Q = vol tau (F J)^-T, f_a = -Q dN_a ---------------
-  T B[9];                                                        // B = (F J)^-1 = dxi/dx
-  const T detFJ = inv3(Jc, B);                                   // det F = det(F J) / det J
+  T B[9];                                                        // B = (8 F J)^-1 = dxi/dx / 8
+  const T detFJ = inv3(Jc, B);                                   // det F = det(8 F J) / (512 det J)
   const T vol = detJ;                                            // Gauss weight 1
-  const T t00 = tau[0] * vol, t11 = tau[1] * vol, t22 = tau[2] * vol;
-  const T t01 = tau[3] * vol, t12 = tau[4] * vol, t02 = tau[5] * vol;
+  const T vol8 = T(8) * detJ;                                    // vol (F J)^-1 = vol8 B
+  const T t00 = tau[0] * vol8, t11 = tau[1] * vol8, t22 = tau[2] * vol8;
+  const T t01 = tau[3] * vol8, t12 = tau[4] * vol8, t02 = tau[5] * vol8;
   T* q = qsm + 12 * lane8;
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
@@ -342,13 +361,14 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
   }
   count_warp(a.cnt, CNT_NR_ACTIVE, valid && (flag & (NR_CONVERGED | NR_FAILED)));
   // the rare events behind one vote: failed return map, both transformations,
-  // det F <= 0 (det F = det(F J) / det J)
+  // det F <= 0 (det F = det(8 F J) / (512 det J))
   const bool negdet = !(detFJ * detJ > T(0));
   if (__any_sync(0xffffffffu, valid && ((flag & (NR_FAILED | NR_BOTH)) || negdet))) {
     count_warp(a.cnt, CNT_NR_FAILED, valid && (flag & NR_FAILED));
     count_warp(a.cnt, CNT_NR_BOTH, valid && (flag & NR_BOTH));
     count_warp(a.cnt, CNT_NEG_DET, valid && negdet);
-    if (valid && negdet) atomicMin(a.cnt + CNT_DETMIN, detmin_key((float)(detFJ / detJ), ec));
+    if (valid && negdet)
+      atomicMin(a.cnt + CNT_DETMIN, detmin_key((float)(detFJ / (T(512) * detJ)), ec));
   }
 }
 
@@ -644,10 +664,14 @@ __global__ void __launch_bounds__(128) k_postproc(ElemArgs<T> a, PostArgs p) {
     U[c] = __ldg(a.u + c * a.npad + nid);
   }
   const int src = (threadIdx.x & 31) & ~7;
+  {
+    T v[6];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    nsm[8 * c + lane8] = (T)(X[c] - __shfl_sync(0xffffffffu, X[c], src));
-    nsm[8 * (3 + c) + lane8] = (T)(U[c] - __shfl_sync(0xffffffffu, U[c], src));
+    for (int c = 0; c < 3; ++c) {
+      v[c] = (T)(X[c] - __shfl_sync(0xffffffffu, X[c], src));
+      v[3 + c] = (T)(U[c] - __shfl_sync(0xffffffffu, U[c], src));
+    }
+    stage_node_rows<T>(nsm, lane8, v);
   }
   const int64_t gp = 8 * ec + lane8;
   double xS = (double)a.sold[gp], F_AS = (double)a.sold[a.sst + gp];

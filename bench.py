@@ -42,6 +42,17 @@ WORKLOADS = {"cantilever": "cantilever_400x40x40_hex08",
              "ensemble": "ensemble_256_specimens_hex08"}
 
 
+def workload_name(workload, div):
+    """The workload's name as run: --div coarsens the cantilever and the
+    cylinder by that factor per direction and cuts the ensemble to 256 / div
+    specimens."""
+    if div == 1:
+        return WORKLOADS[workload]
+    if workload == "ensemble":
+        return f"ensemble_{max(2, 256 // div)}_specimens_hex08"
+    return f"{WORKLOADS[workload]}_coarsened_{div}x"
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -222,7 +233,7 @@ def run_reference(args):
             "ms_per_step": prob.nelem * 8 / base["value"] * 1e3, "higher_is_better": True,
             "scaling": "strong" if (args.workload == "ensemble" and world > 1) else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload], "nelem": prob.nelem, "npoin": prob.npoin,
+            "config": {"workload": workload_name(args.workload, args.div), "nelem": prob.nelem, "npoin": prob.npoin,
                        "gauss_points": prob.nelem * 8, "precision": "fp64 (reference CPU path)",
                        "prestrain": args.prestrain},
             "cpu_baseline": base,
@@ -385,7 +396,7 @@ def main():
                 "scaling": "strong" if sharded else "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if args.precision == "fp32" else "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOADS[args.workload], "nelem": nelem, "npoin": prob.npoin,
+                "config": {"workload": workload_name(args.workload, args.div), "nelem": nelem, "npoin": prob.npoin,
                            "gauss_points": ngp_all, "precision": args.precision,
                            "scatter": args.scatter, "block": block or 128, "variant": variant,
                            "autotuned": bool(tuned), "dtime": prob.dtime,
