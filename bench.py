@@ -42,6 +42,15 @@ WORKLOADS = {"cantilever": "cantilever_400x40x40_hex08",
              "ensemble": "ensemble_256_specimens_hex08"}
 
 
+def default_block(prob, variant):
+    """The element block the library picks when none is given (its context
+    set-up rule): 256 pipelined, else 128 with per-element materials, 64
+    with one."""
+    if variant == "pipe":
+        return 256
+    return 128 if len(prob.props) > 1 else 64
+
+
 def workload_name(workload, div):
     """The workload's name as run: --div coarsens the cantilever and the
     cylinder by that factor per direction and cuts the ensemble to 256 / div
@@ -398,7 +407,7 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": workload_name(args.workload, args.div), "nelem": nelem, "npoin": prob.npoin,
                            "gauss_points": ngp_all, "precision": args.precision,
-                           "scatter": args.scatter, "block": block or 128, "variant": variant,
+                           "scatter": args.scatter, "block": block or default_block(prob, variant), "variant": variant,
                            "autotuned": bool(tuned), "dtime": prob.dtime,
                            "prestrain": args.prestrain,
                            "l2": "working set > L2 (state, nodal arrays and connectivity "

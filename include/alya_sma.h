@@ -99,7 +99,10 @@ typedef struct {
   const double*  fun_tab;   /* concatenated (4, npts) tables (t, vx, vy, vz)   */
   const double*  fext;      /* (3, npoin) nodal load at load factor 1, or NULL */
   int32_t load_fun;         /* table whose vx column scales fext, or -1        */
-  int32_t block;            /* threads per element-kernel block (0 = tuned)    */
+  int32_t block;            /* threads per element-kernel block, a multiple of  *
+                             * 32 in [32, 256]; 0: one tile per block at 64    *
+                             * (one material) or 128 (per-element materials),  *
+                             * the pipelined variant at 256                    */
   int32_t scheme;           /* SMA_SCHEME_CD or SMA_SCHEME_TW                   */
   double  phitw;            /* Tchamwa-Wielgosz phi (0: the reference's 1.033) */
   int32_t variant;          /* element kernel: SMA_VARIANT_*                   */
