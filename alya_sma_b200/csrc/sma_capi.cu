@@ -354,6 +354,8 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance, bool stepping 
   a.beg = beg;
   a.end = end;
   a.mat0 = c->mat0;
+  // one wave of the one-tile kernel: every SM's resident blocks of block / 8 elements
+  a.pf_ahead = (c->variant == SMA_VARIANT_PIPE) ? 0 : (int64_t)c->nsm * c->resident * (c->block / 8);
   a.grav[0] = c->grav[0];
   a.grav[1] = c->grav[1];
   a.grav[2] = c->grav[2];

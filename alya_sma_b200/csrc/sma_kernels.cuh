@@ -126,6 +126,7 @@ struct ElemArgs {
   int has_grav;
   const double* vel;           // SoA [3][npad] velocity for Rayleigh alpha, or null
   MatC mat0;                   // the material when lmate is null (kernel-parameter space)
+  int64_t pf_ahead;            // elements ahead whose connectivity is prefetched to L2 (0: none)
 };
 
 // Shared memory of one element (8 lanes): node data as structure of arrays
@@ -447,7 +448,11 @@ constexpr int ELEM_NARROW_BLOCK = 128;
 // table comes from the constant device array with one material (no block
 // barrier: 2 % faster on the 640 k-element cantilever) and from a shared-
 // memory copy with per-element materials (the constant array was 1.6 %
-// slower on the 2.0 M-element cylinder).
+// slower on the 2.0 M-element cylinder).  With one material each lane also
+// prefetches the connectivity one wave ahead: 4.9 % faster on the
+// cantilever (4.1 % of it with the prefetch compiled in but not taken, from
+// the instruction schedule around it); with per-element materials it was
+// -1.2 % on the cylinder and +1.3 % on the 256-specimen ensemble, so off.
 template <typename T, bool ATOMIC, bool MATS, bool DAMP = false, bool NARROW = false>
 __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
                                   (elem_min_blocks<T, false, MATS, NARROW>())) k_element(ElemArgs<T> a) {
@@ -466,6 +471,14 @@ __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
 
   if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
   if constexpr (MATS) fill_hex8_table<T>(tab_sm);
+  if constexpr (!MATS) {
+    // the connectivity of the element one resident wave ahead, into L2, so
+    // the block that gathers it there starts from an L2 hit
+    if (a.pf_ahead) {
+      const int64_t ep = e + a.pf_ahead;
+      if (ep < a.end) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.lnods + 8 * ep + lane8));
+    }
+  }
 
   const int nid = a.lnods[8 * ec + lane8];
   const double tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
