@@ -101,6 +101,9 @@ def lib():
         L.sma_eval_law160.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p]
+        L.sma_eval_law160_tangent.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p]
         L.sma_set_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.sma_get_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.sma_set_state.argtypes = [C.c_void_p, C.c_void_p]
@@ -359,12 +362,17 @@ def eval_sld_stress_model_160(props, gpgdi, gpsdv, gptmp=None, flagt=0, e_mart=0
     Gauss points: ``gpgdi`` (n, 3, 3) deformation gradients with
     gpgdi[g, i, j] = F(i, j); ``gpsdv`` (n, 3) state of slot TIME_N.  Returns
     (gpstr (n, 3, 3) second Piola stress, new state (n, 3) for slot ITER_K,
-    NR flags (n,)).  Only flagt = 0 (explicit: no tangent) is provided.
+    NR flags (n,)); with flagt = 1 (FP64 only) also gpdds (n, 3, 3, 3, 3),
+    gpdds[g, i, j, k, l] = gpdds(i, j, k, l, igaus), the algorithmic tangent
+    (sld_stress_model_160.f90:118-155, 170-191).
 
     Arrays may be numpy (copied through the device) or torch CUDA tensors
     (used in place)."""
-    if flagt != 0:
-        raise SmaError("only flagt = 0 (explicit, no algorithmic tangent) is provided")
+    if flagt not in (0, 1):
+        raise SmaError("flagt is 0 (stress) or 1 (stress and algorithmic tangent)")
+    if flagt == 1 and precision != "fp64":
+        raise SmaError("the algorithmic tangent is FP64 only: its eps = 1e-5 forward differences "
+                       "are below FP32 resolution")
     import torch
     if not torch.cuda.is_available():
         raise SmaError("eval_sld_stress_model_160 needs a CUDA device")
@@ -383,6 +391,15 @@ def eval_sld_stress_model_160(props, gpgdi, gpsdv, gptmp=None, flagt=0, e_mart=0
     P = torch.empty((n, 9), dtype=torch.float64, device=dev)
     fl = torch.empty(n, dtype=torch.int32, device=dev)
     pr = np.ascontiguousarray(props, dtype=np.float64).reshape(18)
+    if flagt == 1:
+        D = torch.empty((n, 81), dtype=torch.float64, device=dev)
+        _check(lib().sma_eval_law160_tangent(n, _p(pr), float(e_mart), Fc.data_ptr(),
+                                             None if T is None else T.data_ptr(), S0.data_ptr(),
+                                             S1.data_ptr(), P.data_ptr(), D.data_ptr(),
+                                             fl.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        torch.cuda.current_stream().synchronize()
+        gpdds = D.reshape(n, 3, 3, 3, 3).permute(0, 4, 3, 2, 1)     # column-major (i,j,k,l)
+        return P.reshape(n, 3, 3).transpose(1, 2), S1, fl, gpdds
     _check(lib().sma_eval_law160(n, _p(pr), float(e_mart), Fc.data_ptr(),
                                  None if T is None else T.data_ptr(), S0.data_ptr(),
                                  S1.data_ptr(), P.data_ptr(), fl.data_ptr(), PREC[precision],

@@ -1558,6 +1558,19 @@ int32_t sma_eval_law160(int64_t n, const double* props, double e_mart, const dou
   return SMA_OK;
 }
 
+int32_t sma_eval_law160_tangent(int64_t n, const double* props, double e_mart, const double* d_F,
+                                const double* d_tmp, const double* d_sdv_old, double* d_sdv_new,
+                                double* d_pk2, double* d_dds, int32_t* d_nr_flag, void* stream) {
+  if (n < 0) return fail(SMA_ERR_ARG, "n < 0");
+  if (n == 0) return SMA_OK;
+  if (!props || !d_F || !d_sdv_old || !d_sdv_new || !d_pk2 || !d_dds) return fail(SMA_ERR_ARG, "NULL argument");
+  const MatC m = make_mat(props, e_mart, 1.0);
+  k_law_tangent<<<(unsigned)ceil_div(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      n, m, d_F, d_tmp, d_sdv_old, d_sdv_new, d_pk2, d_dds, d_nr_flag);
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

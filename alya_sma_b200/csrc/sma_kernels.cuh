@@ -1210,4 +1210,115 @@ __global__ void k_law_batch(int64_t n, MatC mat, const double* F, const double* 
   if (nr_flag) nr_flag[g] = fl;
 }
 
+// ---------------------------------------------------------------------------
+// batched law with the algorithmic tangent (flagt = 1,
+// sld_stress_model_160.f90:118-155 and 170-191), FP64.  The Kirchhoff stress
+// at F + eps/2 (e_i e_j^T + e_j e_i^T) F, eps = 1e-5 (:61), from the TIME_N
+// state, for the six distinct pairs i <= j (the reference's nine evaluate
+// each off-diagonal pair twice, with identical results); forward
+// differences, the correction of its Eq. 68 with the unperturbed Kirchhoff
+// stress, and the pull-back with F^-1 on all four indices.  Both index pairs
+// are symmetric, so the tangent is carried as a 6 x 6 matrix on
+// (xx yy zz xy yz xz) and expanded to the reference's (3,3,3,3) on output:
+// dds[i + 3j + 9k + 27l + 81g].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int voigt6(int i, int j) {
+  return i == j ? i : (i + j == 1 ? 3 : (i + j == 3 ? 4 : 5));
+}
+__device__ __forceinline__ void voigt6_pair(int v, int& i, int& j) {
+  i = v < 3 ? v : (v == 4 ? 1 : 0);
+  j = v < 3 ? v : (v == 3 ? 1 : 2);
+}
+
+__global__ void __launch_bounds__(128) k_law_tangent(int64_t n, MatC mat, const double* F,
+                                                     const double* tmp, const double* sdv_old,
+                                                     double* sdv_new, double* pk2, double* dds,
+                                                     int32_t* nr_flag) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const double eps = 1.0e-5;
+  const double* Fg = F + 9 * g;
+  double Fm[9], H[9];                                        // Fm[3i+j] = F(i, j)
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      Fm[3 * i + j] = Fg[i + 3 * j];
+      H[3 * i + j] = Fm[3 * i + j] - (i == j ? 1.0 : 0.0);
+    }
+  const double tg = tmp ? tmp[g] : 0.0;
+  const double xs0 = sdv_old[3 * g], fas0 = sdv_old[3 * g + 1], fsa0 = sdv_old[3 * g + 2];
+  double xS = xs0, F_AS = fas0, F_SA = fsa0, tau[6];
+  const int fl = law160_tau<double>(mat, H, tg, xS, F_AS, F_SA, tau);
+  sdv_new[3 * g] = xS;
+  sdv_new[3 * g + 1] = F_AS;
+  sdv_new[3 * g + 2] = F_SA;
+  if (nr_flag) nr_flag[g] = fl;
+
+  // X[p][v]: d tau_v for the perturbation pair p, minus the Eq. 68 term
+  double X[6][6];
+  for (int p = 0; p < 6; ++p) {
+    int i, j;
+    voigt6_pair(p, i, j);
+    double Hp[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        const double a = (r == i ? Fm[3 * j + c] : 0.0) + (r == j ? Fm[3 * i + c] : 0.0);
+        Hp[3 * r + c] = H[3 * r + c] + 0.5 * eps * a;
+      }
+    double xs = xs0, fas = fas0, fsa = fsa0, tp[6];
+    law160_tau<double>(mat, Hp, tg, xs, fas, fsa, tp);
+    for (int v = 0; v < 6; ++v) {
+      int c, d;
+      voigt6_pair(v, c, d);
+      const double corr = (i == c ? tau[voigt6(d, j)] : 0.0) + (c == j ? tau[voigt6(i, d)] : 0.0) +
+                          (i == d ? tau[voigt6(c, j)] : 0.0) + (d == j ? tau[voigt6(i, c)] : 0.0);
+      X[p][v] = (tp[v] - tau[v]) / eps - 0.5 * corr;
+    }
+  }
+
+  // pull-back: G = Q X Q^T with Q[s][w] = sum over (m, n) of pair w of
+  // F^-1(i, m) F^-1(j, n), (i, j) the pair s
+  double Fi[9];
+  inv3(Fm, Fi);
+  double Q[6][6];
+  for (int s = 0; s < 6; ++s) {
+    int i, j;
+    voigt6_pair(s, i, j);
+    for (int w = 0; w < 6; ++w) {
+      int m, nn;
+      voigt6_pair(w, m, nn);
+      Q[s][w] = Fi[3 * i + m] * Fi[3 * j + nn] + (m != nn ? Fi[3 * i + nn] * Fi[3 * j + m] : 0.0);
+    }
+  }
+  double Y[6][6];                                            // Y = X Q^T
+  for (int w = 0; w < 6; ++w)
+    for (int t = 0; t < 6; ++t) {
+      double acc = 0.0;
+      for (int u = 0; u < 6; ++u) acc += X[w][u] * Q[t][u];
+      Y[w][t] = acc;
+    }
+  double* out = dds + 81 * g;
+  for (int s = 0; s < 6; ++s)
+    for (int t = 0; t < 6; ++t) {
+      double acc = 0.0;
+      for (int w = 0; w < 6; ++w) acc += Q[s][w] * Y[w][t];
+      int i, j, k, l;
+      voigt6_pair(s, i, j);
+      voigt6_pair(t, k, l);
+      out[i + 3 * j + 9 * k + 27 * l] = acc;
+      out[j + 3 * i + 9 * k + 27 * l] = acc;
+      out[i + 3 * j + 9 * l + 27 * k] = acc;
+      out[j + 3 * i + 9 * l + 27 * k] = acc;
+    }
+
+  // S = F^-1 tau F^-T (eval_sld_stress_model_160, :159-168)
+  const double tf[9] = {tau[0], tau[3], tau[5], tau[3], tau[1], tau[4], tau[5], tau[4], tau[2]};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) acc += Fi[3 * i + k] * Fi[3 * j + l] * tf[3 * k + l];
+      pk2[9 * g + i + 3 * j] = acc;
+    }
+}
+
 }  // namespace sma

@@ -182,6 +182,15 @@ int32_t sma_eval_law160(int64_t n, const double* props, double e_mart,
                         const double* d_sdv_old, double* d_sdv_new, double* d_pk2,
                         int32_t* d_nr_flag, int32_t precision, void* stream);
 
+/* The same plugin with flagt = 1 (FP64): also the algorithmic tangent
+ * d_dds (81n), dds[i + 3j + 9k + 27l + 81g] = gpdds(i,j,k,l,igaus), from
+ * eps = 1e-5 forward differences of the Kirchhoff stress, corrected and
+ * pulled back with F^-1 (sld_stress_model_160.f90:118-155, 170-191). */
+int32_t sma_eval_law160_tangent(int64_t n, const double* props, double e_mart,
+                                const double* d_F, const double* d_tmp,
+                                const double* d_sdv_old, double* d_sdv_new, double* d_pk2,
+                                double* d_dds, int32_t* d_nr_flag, void* stream);
+
 /* Element loop that allocates nothing.  No counterpart in the reference:
  * it exists for callers that cannot allocate device memory themselves
  * through the CUDA runtime (a Fortran host whose device arrays belong to an

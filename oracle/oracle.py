@@ -112,6 +112,29 @@ def law160_batch(props, F, sdv_old, tmp=None, e_mart=0.0, dtype=np.float64):
     return pk2, sn, fl
 
 
+def law160_tangent_batch(props, F, sdv_old, tmp=None, e_mart=0.0, dtype=np.float64):
+    """Batched law with the algorithmic tangent (flagt = 1): F (n,9) column-major.
+
+    Returns (pk2 (n,9), sdv_new (n,3), dds (n,81) with dds[g, i+3j+9k+27l] =
+    gpdds(i,j,k,l), flags)."""
+    npt, ct, sfx = _f(dtype)
+    props = np.ascontiguousarray(props, dtype=npt)
+    F = np.ascontiguousarray(F, dtype=npt).reshape(-1, 9)
+    n = F.shape[0]
+    so = np.ascontiguousarray(sdv_old, dtype=npt).reshape(n, 3)
+    sn = np.zeros((n, 3), npt)
+    pk2 = np.zeros((n, 9), npt)
+    dds = np.zeros((n, 81), npt)
+    fl = np.zeros(n, np.int32)
+    t = None if tmp is None else np.ascontiguousarray(tmp, dtype=npt)
+    fn = getattr(lib(), "orc_law160_tangent_batch" + sfx)
+    fn.argtypes = [C.c_int64, C.POINTER(ct), ct, C.POINTER(ct), C.POINTER(ct), C.POINTER(ct),
+                   C.POINTER(ct), C.POINTER(ct), C.POINTER(ct), C.POINTER(C.c_int32)]
+    fn(n, _ptr(props, ct), ct(e_mart), _ptr(F, ct), _ptr(t, ct), _ptr(so, ct), _ptr(sn, ct),
+       _ptr(pk2, ct), _ptr(dds, ct), _ptr(fl, C.c_int32))
+    return pk2, sn, dds, fl
+
+
 def color_elements(lnods, npoin):
     lnods = np.ascontiguousarray(lnods, dtype=np.int32)
     nelem = lnods.shape[0]

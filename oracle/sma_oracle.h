@@ -60,6 +60,9 @@ extern "C" {
   void orc_law160_batch##S(int64_t n, const T props[18], T e_mart, const T* F,      \
                            const T* tmp, const T* sdv_old, T* sdv_new, T* pk2,      \
                            int32_t* nr_flag);                                       \
+  void orc_law160_tangent_batch##S(int64_t n, const T props[18], T e_mart,          \
+                                   const T* F, const T* tmp, const T* sdv_old,      \
+                                   T* sdv_new, T* pk2, T* dds, int32_t* nr_flag);   \
   void orc_hex8_gauss##S(T posgp[24], T weigp[8]);                                  \
   void orc_hex8_shape##S(T s, T t, T z, T shapf[8], T deriv[24]);                   \
   T    orc_hex8_celen##S(const T elcod[24]);                                        \

@@ -384,6 +384,76 @@ void FN(orc_law160_batch)(int64_t n, const REAL props[18], REAL e_mart, const RE
   }
 }
 
+/* Batched law with the algorithmic tangent (flagt = 1), following
+ * eval_sld_stress_model_160 (sld_stress_model_160.f90:118-155, 170-191):
+ * for every (i, j) the Kirchhoff stress at F + eps/2 (e_i e_j^T F +
+ * e_j e_i^T F), eps = 1e-5 (:61), each from the TIME_N state (:130-131);
+ * forward differences (:137); the correction of its Ref_D Eq. 68 with the
+ * unperturbed Kirchhoff stress (:140-153, car_basis = identity); the pull-
+ * back with F^-1 on all four indices (:170-191).  Outputs as
+ * orc_law160_batch plus dds[i + 3j + 9k + 27l + 81g] = gpdds(i,j,k,l,g). */
+void FN(orc_law160_tangent_batch)(int64_t n, const REAL props[18], REAL e_mart,
+                                  const REAL* F, const REAL* tmp, const REAL* sdv_old,
+                                  REAL* sdv_new, REAL* pk2, REAL* dds, int32_t* nr_flag)
+{
+  const REAL eps = (REAL)1.0e-5;
+  for (int64_t g = 0; g < n; ++g) {
+    const REAL* Fg = F + 9 * g;
+    const REAL tg = tmp ? tmp[g] : (REAL)0;
+    REAL Finv[9], tau[9], sdv[3], D[81];
+    FN(inv3x3)(Fg, Finv);
+    for (int c = 0; c < 3; ++c) sdv[c] = sdv_old[3 * g + c];
+    const int fl = FN(orc_law160_kirchhoff)(props, e_mart, Fg, tg, sdv, tau);
+    for (int c = 0; c < 3; ++c) sdv_new[3 * g + c] = sdv[c];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        REAL Fp[9], tp[9], sp[3];
+        /* (e_i e_j^T F)(r, c) = delta_ri F(j, c) */
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) {
+            const REAL a = (r == i ? M3(Fg, j, c) : (REAL)0) + (r == j ? M3(Fg, i, c) : (REAL)0);
+            M3(Fp, r, c) = M3(Fg, r, c) + (REAL)0.5 * eps * a;
+          }
+        for (int c = 0; c < 3; ++c) sp[c] = sdv_old[3 * g + c];
+        FN(orc_law160_kirchhoff)(props, e_mart, Fp, tg, sp, tp);
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l)
+            D[i + 3 * j + 9 * k + 27 * l] = (M3(tp, k, l) - M3(tau, k, l)) / eps;
+      }
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        for (int c = 0; c < 3; ++c)
+          for (int d = 0; d < 3; ++d)
+            D[a + 3 * b + 9 * c + 27 * d] -= (REAL)0.5 *
+                ((a == c ? M3(tau, d, b) : (REAL)0) + (c == b ? M3(tau, a, d) : (REAL)0) +
+                 (a == d ? M3(tau, c, b) : (REAL)0) + (d == b ? M3(tau, a, c) : (REAL)0));
+    REAL* out = dds + 81 * g;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) {
+            REAL s = 0;
+            for (int m = 0; m < 3; ++m)
+              for (int nn = 0; nn < 3; ++nn)
+                for (int p = 0; p < 3; ++p)
+                  for (int q = 0; q < 3; ++q)
+                    s = s + M3(Finv, i, m) * M3(Finv, j, nn) * M3(Finv, k, p) * M3(Finv, l, q) *
+                                D[m + 3 * nn + 9 * p + 27 * q];
+            out[i + 3 * j + 9 * k + 27 * l] = s;
+          }
+    REAL* S = pk2 + 9 * g;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        REAL s = 0;
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l)
+            s = s + M3(Finv, i, k) * M3(Finv, j, l) * M3(tau, k, l);
+        M3(S, i, j) = s;
+      }
+    if (nr_flag) nr_flag[g] = fl;
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 /* HEX08 reference element                                                   */
 /* ------------------------------------------------------------------------ */
