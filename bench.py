@@ -259,11 +259,12 @@ def main():
     import torch
     import alya_sma_b200 as sma
     rank, world, local = dist_env()
+    torch.cuda.set_device(local)                              # before NCCL binds the rank's device
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     prob = build_problem(args.workload, args.div, rank, world)
     nelem, ngp = prob.nelem, prob.nelem * 8
     sharded = args.workload == "ensemble" and world > 1       # strong scaling: fixed total work
@@ -311,8 +312,8 @@ def main():
     launches = solid.kernel_launches - l0
     ms = e0.elapsed_time(e1)
     ngp_all = world * ngp                                      # replicas: the same mesh per rank
+    from alya_sma_b200 import dist as D                       # (identity on one rank)
     if world > 1:
-        from alya_sma_b200 import dist as D
         ms = D.max_over_ranks(ms, "cuda")                      # the slowest rank sets the time
         if sharded:
             ngp_all = int(D.sum_over_ranks(ngp, "cuda"))       # each specimen counted once
@@ -372,7 +373,10 @@ def main():
             extras["plain_fp64"] = {"value": v64, "unit": "GP-updates/s", "steps": k64}
             extras["speedup_vs_plain_fp64"] = round(value / world / v64, 3)
             s64.close()
-        # e2e: the element-loop C-ABI call with pinned host buffers
+    if not args.no_extras:
+        # e2e on every rank: the element-loop C-ABI call with pinned host
+        # buffers, host copies inside the timed region; the job's Gauss points
+        # over the slowest rank's time
         npoin = prob.npoin
         hd = torch.zeros((npoin, 3), dtype=torch.float64).pin_memory()
         hr = torch.zeros((npoin, 3), dtype=torch.float64).pin_memory()
@@ -384,13 +388,13 @@ def main():
             sma._check(L.sma_assemble(ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
             solid.end_step()
         ke = max(10, args.steps // 20)
-        torch.cuda.synchronize()
+        barrier()
         t0 = time.perf_counter()
         for _ in range(ke):
             sma._check(L.sma_assemble(ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
             solid.end_step()
-        te = time.perf_counter() - t0
-        extras["e2e"] = {"value": ngp * ke / te, "unit": "GP-updates/s",
+        te = D.max_over_ranks(time.perf_counter() - t0, "cuda")
+        extras["e2e"] = {"value": ngp_all * ke / te, "unit": "GP-updates/s",
                          "h2d_bytes_per_step": 3 * npoin * 8, "d2h_bytes_per_step": 3 * npoin * 8,
                          "boundary": "sma_assemble (element loop, host displ in, host rhsid out)"}
         if world == 1:
