@@ -67,6 +67,20 @@ def test_null_arguments_are_errors():
     assert L.sma_ctx_create(None, None, None, None) == -1
     assert L.sma_explicit_step(None, 1) == -1
     assert L.sma_eval_law160(-1, None, C.c_double(0.0), None, None, None, None, None, None, 0, None) == -1
+    assert L.sma_eval_law160_tangent(-1, None, C.c_double(0.0), None, None, None, None, None, None,
+                                     None, None) == -1
+    props = np.ascontiguousarray(P.nitinol_props(**P.NITI))
+    assert L.sma_eval_law160_tangent(0, props.ctypes.data, C.c_double(0.0), None, None, None, None,
+                                     None, None, None, None) == 0                 # n = 0: nothing to do
+    assert L.sma_eval_law160_tangent(4, props.ctypes.data, C.c_double(0.0), None, None, None, None,
+                                     None, None, None, None) == -1                # NULL device arrays
+
+
+def test_rejects_empty_mesh():
+    p = _prob()
+    p.lnods = p.lnods[:0]
+    with pytest.raises(sma.SmaError, match="empty mesh"):
+        sma.ExplicitSolid(p)
 
 
 def test_no_device_is_an_error_not_a_fallback():

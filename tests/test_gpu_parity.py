@@ -224,6 +224,51 @@ def test_every_block_width_matches_oracle(oracle, bar, mesh, precision):
         assert np.abs(rhs[128] - rhs[256]).max() <= 1e-12 * scale
 
 
+def _first_elements(p, k):
+    """The first k elements of p with their nodes renumbered."""
+    nodes = np.unique(p.lnods[:k])
+    remap = -np.ones(p.npoin, np.int64)
+    remap[nodes] = np.arange(nodes.size)
+    return P.Problem(coord=p.coord[nodes], lnods=remap[p.lnods[:k]].astype(np.int32), props=p.props,
+                     e_mart=p.e_mart, densi=p.densi, fixno=p.fixno[nodes], bcfun=p.bcfun[nodes],
+                     fun_npts=p.fun_npts, fun_smooth=p.fun_smooth, fun_tab=p.fun_tab,
+                     fext=None if p.fext is None else p.fext[nodes], load_fun=p.load_fun,
+                     dtime=p.dtime, nsteps=p.nsteps)
+
+
+@pytest.mark.parametrize("k", [1, 3, 9])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("fp32", 1e-3)])
+def test_meshes_smaller_than_a_tile(oracle, bar, k, precision, tol):
+    """1, 3 and 9 elements: fewer than the 8 elements of one default block,
+    and one ragged tile past it (the lanes of missing elements gather a valid
+    element's nodes but neither write state nor scatter forces)."""
+    q = _first_elements(bar, k)
+    assert q.nelem == k
+    u = deformed(q, seed=k, strain=0.03)
+    u[q.fixno == 1] = 0.0
+    o = oracle.Problem(q)
+    ro = o.assemble(u)
+    o.end_step()
+    g = sma.ExplicitSolid(q, precision=precision)
+    rg = g.assemble(u)
+    g.end_step()
+    scale = np.abs(ro["finte"]).max()
+    for key in ("rhsid", "finte"):
+        assert np.abs(rg[key] - ro[key]).max() <= tol * scale, key
+    np.testing.assert_allclose(rg["vmass"], ro["vmass"], rtol=1e-13)
+    assert np.abs(g.state[:, 1, :, 0] - o.sdv[:, 1, :, 0]).max() < (1e-8 if precision == "fp64" else 2e-3)
+    # free vibration from the deformed state
+    o2 = oracle.Problem(q)
+    o2.displ[:] = u
+    o2.run(q.dtime, 30)
+    g2 = sma.ExplicitSolid(q, precision=precision)
+    g2.set("displ", u)
+    g2.step(30)
+    ud, ud_ref = g2.get("displ"), o2.displ
+    assert np.abs(ud - ud_ref).max() <= (1e-6 if precision == "fp64" else 1e-3) * np.abs(ud_ref).max()
+    assert g2.counters()["nonfinite"] == 0
+
+
 def test_colour_scatter_is_deterministic(bar):
     runs = []
     for _ in range(2):
