@@ -297,6 +297,8 @@ def main():
     ckpt = os.path.join(tempfile.mkdtemp(prefix="sma_bench_"), f"window_r{rank}.bin")
     solid.save(ckpt)
 
+    solid.counters(reset=True)                 # the window's physics, counted by the kernels
+
     # ---- timed region: K device-resident steps (CUDA graphs) ---------------
     clocks = Clocks(local)
     barrier()
@@ -311,6 +313,10 @@ def main():
     ck = clocks.stop()
     launches = solid.kernel_launches - l0
     ms = e0.elapsed_time(e1)
+    cnt = solid.counters()
+    physics = {"gauss_points_in_return_map_per_step": round(cnt["nr_active"] / args.steps),
+               "return_map_failures": cnt["nr_failed"], "det_F_nonpositive": cnt["neg_det"],
+               "nonfinite": cnt["nonfinite"]}
     ngp_all = world * ngp                                      # replicas: the same mesh per rank
     from alya_sma_b200 import dist as D                       # (identity on one rank)
     if world > 1:
@@ -418,7 +424,7 @@ def main():
                                  f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",
                            "parallelism": (f"specimens sharded over {world} GPUs (no exchange)" if sharded
                                            else f"replicas x{world}" if world > 1 else "single GPU")},
-                "roofline": roofline, "gpu_launches": launches, "clocks": ck}
+                "roofline": roofline, "gpu_launches": launches, "clocks": ck, "physics": physics}
         line.update(extras)
         print(json.dumps(line))
     solid.close()
