@@ -423,8 +423,10 @@ __device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC
 // threads, the one-tile default; else 256) and the minimum resident blocks,
 // which cap registers at 65536 / (threads x blocks).  Measured on B200 over
 // fixed step windows of the one-tile kernel:
-//   FP32, one material: 80 registers at either width (6 x 128 or 3 x 256,
-//     24 warps per SM, no spills);
+//   FP32, one material: 72 registers narrow (7 x 128: 28 warps per SM at
+//     64-thread blocks, 32 B of spills), which beat 80 (24 warps) by 2.3 %
+//     and 64 (32 warps, 56 B of spills) by 0.7 % on the 640 k-element
+//     cantilever once the connectivity prefetch was in; 80 wide (3 x 256);
 //   FP32 with per-element materials, and FP64: 96 registers at 5 x 128 (20
 //     warps, 24-120 bytes of spills) beat 128 registers at 16 warps by 2-8%
 //     (FP64 cantilever 0.399 -> 0.367 ms, FP32 ensemble 1.643 -> 1.611 ms);
@@ -435,7 +437,7 @@ __device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC
 template <typename T, bool PIPE, bool MATS, bool NARROW = false>
 constexpr int elem_min_blocks() {
   if (PIPE) return 2;
-  if (NARROW) return (sizeof(T) == 4 && !MATS) ? 6 : 5;
+  if (NARROW) return (sizeof(T) == 4 && !MATS) ? 7 : 5;
   return (sizeof(T) == 4 && !MATS) ? 3 : 2;
 }
 constexpr int ELEM_NARROW_BLOCK = 128;
