@@ -427,17 +427,19 @@ __device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC
 //     64-thread blocks, 32 B of spills), which beat 80 (24 warps) by 2.3 %
 //     and 64 (32 warps, 56 B of spills) by 0.7 % on the 640 k-element
 //     cantilever once the connectivity prefetch was in; 80 wide (3 x 256);
-//   FP32 with per-element materials, and FP64: 96 registers at 5 x 128 (20
-//     warps, 24-120 bytes of spills) beat 128 registers at 16 warps by 2-8%
-//     (FP64 cantilever 0.399 -> 0.367 ms, FP32 ensemble 1.643 -> 1.611 ms);
-//     80 registers at 24 warps lost 10% on the ensemble, 168 registers at 12
-//     warps lost 17% on the FP64 cantilever;
+//   FP64, one material: 80 registers narrow (6 x 128, 24 warps, 80 B of
+//     spills): -4.7 % against 96 on the cantilever;
+//   FP32 with per-element materials, and FP64 with per-element materials:
+//     96 registers at 5 x 128 (20 warps; FP32 92 without spills) beat 128
+//     registers at 16 warps by 2-8 % (FP32 ensemble 1.643 -> 1.611 ms);
+//     80 registers lost 18 % on the FP32 ensemble and were even in FP64,
+//     168 registers at 12 warps lost 17 % on the FP64 cantilever;
 //   256-thread blocks with per-element materials or FP64, and the pipelined
 //     kernel: 2 x 256 (128 registers).
 template <typename T, bool PIPE, bool MATS, bool NARROW = false>
 constexpr int elem_min_blocks() {
   if (PIPE) return 2;
-  if (NARROW) return (sizeof(T) == 4 && !MATS) ? 7 : 5;
+  if (NARROW) return MATS ? 5 : (sizeof(T) == 4 ? 7 : 6);
   return (sizeof(T) == 4 && !MATS) ? 3 : 2;
 }
 constexpr int ELEM_NARROW_BLOCK = 128;
