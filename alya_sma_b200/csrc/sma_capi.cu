@@ -848,15 +848,16 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   else
     c->variant = (run->variant == SMA_VARIANT_PLAIN) ? SMA_VARIANT_PLAIN : SMA_VARIANT_PIPE;
   // default block, measured on B200 over fixed step windows: the one-tile
-  // kernel at 64 threads with one material (finer scheduling at the same
-  // warps per SM, no block barrier: -1.4 % FP32, -1.6 % FP64 element time on
-  // the 640 k-element cantilever), at 128 with per-element materials (their
-  // table fill and barrier amortise over more elements: -0.7 % FP32 / -2.5 %
+  // kernel at 32 threads (one warp, 4 elements) with one material (finer
+  // scheduling at the same warps per SM, no block barrier: against 128,
+  // -2.1 % FP32 and -1.9 % FP64 element time on the 640 k-element
+  // cantilever), at 128 with per-element materials (their table fill and
+  // barrier amortise over more elements: against 64, -0.7 % FP32 / -2.5 %
   // FP64 on the 3.73 M-element ensemble, -3.1 % FP64 on the 2.0 M-element
   // cylinder); 256 for the pipelined kernel
   const bool per_element_mats = mesh->lmate && mat->nmate > 1;
   c->block = run->block ? run->block
-                        : (c->variant == SMA_VARIANT_PIPE ? 256 : (per_element_mats ? 128 : 64));
+                        : (c->variant == SMA_VARIANT_PIPE ? 256 : (per_element_mats ? 128 : 32));
   c->nsm = prop.multiProcessorCount;
   c->nelem = mesh->nelem;
   c->npoin = mesh->npoin;

@@ -15,9 +15,9 @@ import json
 import math
 import os
 
-CANDIDATES = ((64, "atomic", "plain"), (128, "atomic", "plain"), (256, "atomic", "plain"),
-              (128, "atomic", "pipe"), (256, "atomic", "pipe"), (64, "color", "plain"),
-              (256, "color", "pipe"))
+CANDIDATES = ((32, "atomic", "plain"), (64, "atomic", "plain"), (128, "atomic", "plain"),
+              (256, "atomic", "plain"), (128, "atomic", "pipe"), (256, "atomic", "pipe"),
+              (64, "color", "plain"), (256, "color", "pipe"))
 
 
 def cache_path() -> str:

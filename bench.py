@@ -44,11 +44,11 @@ WORKLOADS = {"cantilever": "cantilever_400x40x40_hex08",
 
 def default_block(prob, variant):
     """The element block the library picks when none is given (its context
-    set-up rule): 256 pipelined, else 128 with per-element materials, 64
+    set-up rule): 256 pipelined, else 128 with per-element materials, 32
     with one."""
     if variant == "pipe":
         return 256
-    return 128 if len(prob.props) > 1 else 64
+    return 128 if len(prob.props) > 1 else 32
 
 
 def workload_name(workload, div):

@@ -100,7 +100,7 @@ typedef struct {
   const double*  fext;      /* (3, npoin) nodal load at load factor 1, or NULL */
   int32_t load_fun;         /* table whose vx column scales fext, or -1        */
   int32_t block;            /* threads per element-kernel block, a multiple of  *
-                             * 32 in [32, 256]; 0: one tile per block at 64    *
+                             * 32 in [32, 256]; 0: one tile per block at 32    *
                              * (one material) or 128 (per-element materials),  *
                              * the pipelined variant at 256                    */
   int32_t scheme;           /* SMA_SCHEME_CD or SMA_SCHEME_TW                   */

@@ -210,7 +210,7 @@ def test_every_block_width_matches_oracle(oracle, bar, mesh, precision):
     scale = np.abs(ro["finte"]).max()
     tol, tol_x = (1e-8, 1e-8) if precision == "fp64" else (1e-3, 2e-3)
     rhs = {}
-    for block in (64, 128, 192, 256):
+    for block in (32, 64, 128, 192, 256):
         g = sma.ExplicitSolid(p, precision=precision, scatter="color", block=block)
         rg = g.assemble(u)
         g.end_step()
