@@ -71,7 +71,8 @@ _lib = None
 
 def header_functions() -> list[str]:
     """Names of every entry point declared in include/alya_sma.h."""
-    txt = open(HEADER).read()
+    with open(HEADER) as fh:
+        txt = fh.read()
     return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\*\s]+?\b(sma_\w+)\s*\(", txt, re.M)))
 
 
@@ -105,6 +106,11 @@ def lib():
                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_void_p, C.c_void_p]
         L.sma_set_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.sma_step_prologue.argtypes = [C.c_void_p]
+        L.sma_step_elements.argtypes = [C.c_void_p]
+        L.sma_step_nodes.argtypes = [C.c_void_p, C.c_int32]
+        L.sma_gather_residual.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        L.sma_scatter_residual.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.sma_get_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.sma_set_state.argtypes = [C.c_void_p, C.c_void_p]
         L.sma_get_state.argtypes = [C.c_void_p, C.c_void_p]
@@ -233,7 +239,8 @@ class ExplicitSolid:
         return out
 
     def set(self, field, arr):
-        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.npoin, 3)
+        n = (self.npoin,) if field == "vmass" else (self.npoin, 3)
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(n)
         _check(lib().sma_set_nodal(self._ctx, FIELD[field], _p(a)))
 
     @property

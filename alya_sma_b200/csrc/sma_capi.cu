@@ -1022,6 +1022,64 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   return SMA_OK;
 }
 
+// the explicit step in parts, for partitioned meshes (the caller sums the
+// interface residual between sma_step_elements and sma_step_nodes)
+int32_t sma_step_prologue(sma_ctx* c) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (!(c->dtime > 0.0)) return fail(SMA_ERR_STATE, "dtime not set");
+  CU(cudaSetDevice(c->dev));
+  if (c->nwit > 0) CU(cudaMemsetAsync(c->d_wrow, 0, sizeof(int), c->stream));
+  k_advance_time<<<1, 1, 0, c->stream>>>(c->d_ts, c->d_ft);
+  c->launches++;
+  return launch_nodal(c, 0);
+}
+
+int32_t sma_step_elements(sma_ctx* c) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc = launch_elements(c, true);
+  if (rc) return rc;
+  c->cur ^= 1;
+  if ((rc = launch_witness(c))) return rc;
+  if (c->damp && c->energy && (rc = launch_rayleigh(c, damp_velocity(c, true)))) return rc;
+  return SMA_OK;
+}
+
+int32_t sma_step_nodes(sma_ctx* c, int32_t last) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc = launch_nodal(c, last ? 2 : 1);
+  if (rc) return rc;
+  if (last) CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+int32_t sma_gather_residual(sma_ctx* c, int32_t n, const int32_t* d_nodes, double* d_rows) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (n < 0) return fail(SMA_ERR_ARG, "n < 0");
+  if (n == 0) return SMA_OK;
+  if (!d_nodes || !d_rows) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  k_gather_rows<<<(unsigned)ceil_div(n, 256), 256, 0, c->stream>>>(c->d_f, c->npad, c->npoin, n, d_nodes,
+                                                                    d_rows);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+int32_t sma_scatter_residual(sma_ctx* c, int32_t n, const int32_t* d_nodes, const double* d_rows) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (n < 0) return fail(SMA_ERR_ARG, "n < 0");
+  if (n == 0) return SMA_OK;
+  if (!d_nodes || !d_rows) return fail(SMA_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(c->dev));
+  k_scatter_rows<<<(unsigned)ceil_div(n, 256), 256, 0, c->stream>>>(c->d_f, c->npad, c->npoin, n, d_nodes,
+                                                                     d_rows);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
 int32_t sma_explicit_step(sma_ctx* c, int32_t nsteps) {
   if (!c) return fail(SMA_ERR_ARG, "NULL context");
   if (nsteps < 0) return fail(SMA_ERR_ARG, "nsteps < 0");
@@ -1201,6 +1259,21 @@ int32_t sma_gauss_fields(sma_ctx* c, double* gpgdi, double* gppio, double* gpdet
 
 int32_t sma_set_nodal(sma_ctx* c, int32_t field, const double* host) {
   if (!c || !host) return fail(SMA_ERR_ARG, "NULL argument");
+  if (field == SMA_FIELD_VMASS) {
+    // a partitioned mesh's interface nodes take the mass summed over the
+    // sub-meshes that share them
+    for (int p = 0; p < c->npoin; ++p)
+      if (!(host[p] > 0.0)) return fail(SMA_ERR_ARG, "lumped mass must be positive");
+    std::vector<double> invm(c->npad, 0.0);
+    for (int p = 0; p < c->npoin; ++p) {
+      c->vmass[p] = host[p];
+      invm[p] = 1.0 / host[p];
+    }
+    CU(cudaSetDevice(c->dev));
+    CU(cudaStreamSynchronize(c->stream));
+    CU(cudaMemcpy(c->d_invm, invm.data(), invm.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return SMA_OK;
+  }
   double* dst = nullptr;
   switch (field) {
     case SMA_FIELD_DISPL: dst = c->d_u; break;

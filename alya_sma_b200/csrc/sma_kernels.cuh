@@ -1171,6 +1171,26 @@ __global__ void k_state_out(double* host_layout, const int32_t* perm, const T* s
   }
 }
 
+// residual rows of selected nodes (interface nodes of a partitioned mesh):
+// rows[3i + c] = f[c][nodes[i]]; ids outside [0, npoin) read as zero and are
+// never written
+__global__ void k_gather_rows(const double* f, int64_t npad, int64_t npoin, int32_t n,
+                              const int32_t* nodes, double* rows) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t p = nodes[i];
+  const bool ok = p >= 0 && p < npoin;
+  for (int c = 0; c < 3; ++c) rows[3 * i + c] = ok ? f[c * npad + p] : 0.0;
+}
+__global__ void k_scatter_rows(double* f, int64_t npad, int64_t npoin, int32_t n, const int32_t* nodes,
+                               const double* rows) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t p = nodes[i];
+  if (p < 0 || p >= npoin) return;
+  for (int c = 0; c < 3; ++c) f[c * npad + p] = rows[3 * i + c];
+}
+
 // ---------------------------------------------------------------------------
 // batched law (material-plugin boundary): F column-major (9n) -> PK2 (9n)
 // ---------------------------------------------------------------------------

@@ -54,7 +54,7 @@ extern "C" {
 #define SMA_FIELD_VELOC     1
 #define SMA_FIELD_ACCEL     2
 #define SMA_FIELD_RHSID     3   /* last assembled residual f_ext - f_int       */
-#define SMA_FIELD_VMASS     4   /* lumped mass, (npoin) only                   */
+#define SMA_FIELD_VMASS     4   /* lumped mass, (npoin) only; settable (> 0)   */
 
 /* counters (sma_counters.c[k]) accumulated since creation / reset */
 #define SMA_CNT_NR_ACTIVE   0   /* law evaluations with a transformation active */
@@ -218,6 +218,22 @@ int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int32_t* d_lnod
 
 /* host <-> context data */
 int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);
+
+/* Partitioned meshes: one sub-mesh per GPU, nodes on the cut shared by the
+ * sub-meshes.  sma_explicit_step in its parts, so the caller can sum the
+ * residual of shared nodes between the element loop and the nodal update --
+ * the reference's rhsmod -> pararr('SLX') exchange (sld_matrix.f90:274-281)
+ * -- after summing their lumped mass once (sma_set_nodal SMA_FIELD_VMASS).
+ * n steps: sma_step_prologue, then n times sma_step_elements, the exchange,
+ * sma_step_nodes(last = final step).  The same kernels as sma_explicit_step,
+ * without its graphs; witness and energy records stay per sub-mesh.
+ * sma_gather/scatter_residual copy the residual rows of n nodes (device ids,
+ * 0-based) to/from a device buffer (3, n) on the context stream. */
+int32_t sma_step_prologue(sma_ctx* ctx);
+int32_t sma_step_elements(sma_ctx* ctx);
+int32_t sma_step_nodes(sma_ctx* ctx, int32_t last);
+int32_t sma_gather_residual(sma_ctx* ctx, int32_t n, const int32_t* d_nodes, double* d_rows);
+int32_t sma_scatter_residual(sma_ctx* ctx, int32_t n, const int32_t* d_nodes, const double* d_rows);
 int32_t sma_get_nodal(sma_ctx* ctx, int32_t field, double* host);
 int32_t sma_set_state(sma_ctx* ctx, const double* host_sdv);   /* (3,8,2,nelem) */
 int32_t sma_get_state(sma_ctx* ctx, double* host_sdv);

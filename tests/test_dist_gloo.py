@@ -40,7 +40,7 @@ def _worker(rank, world, port, out):
 def test_two_gloo_ranks_shard_ensemble_and_reduce():
     world = 2
     port = _free_port()
-    with mp.Manager() as man:
+    with mp.get_context("spawn").Manager() as man:   # no fork of a threaded process
         out = man.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)

@@ -61,7 +61,8 @@ def test_data1_transitions_reproduced(oracle):
 
 
 def test_data1_envelope(oracle):
-    env = json.load(open(os.path.join(GOLD, "data1_envelope.json")))
+    with open(os.path.join(GOLD, "data1_envelope.json")) as fh:
+        env = json.load(fh)
     assert env["F_max"] <= env["Rf_AS"]
     assert -1e-12 <= env["xS_min"] and env["xS_max"] <= 1.0
     assert env["transitions_within_1e9"] == env["transitions"]
