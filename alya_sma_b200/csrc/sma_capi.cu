@@ -1728,9 +1728,11 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   a.end = nelem;
   a.has_grav = 0;
   a.vel = nullptr;
-  const int block = 256, epb = block / 8;
+  // the one-material narrow instance at one-warp blocks, as a context
+  // with one material runs it by default
+  const int block = 32, epb = block / 8;
   const size_t smem = element_smem_bytes<T>(block, false);      // below the 48 KB default
-  k_element<T, true, false><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
+  k_element<T, true, false, false, true><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
   k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
   CU(cudaGetLastError());
   return SMA_OK;
@@ -1760,10 +1762,10 @@ extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int3
     // set-up, once per device, with that device current
     void* p = nullptr;
     CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    CU(cudaFuncSetAttribute(k_element<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            48 * 1024));
-    CU(cudaFuncSetAttribute(k_element<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            48 * 1024));
+    CU(cudaFuncSetAttribute(k_element<double, true, false, false, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024));
+    CU(cudaFuncSetAttribute(k_element<float, true, false, false, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024));
     g_noalloc_ptr[dev] = (unsigned char*)p;
   }
   unsigned char* base = g_noalloc_ptr[dev];
