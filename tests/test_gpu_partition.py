@@ -44,6 +44,21 @@ def test_partitioned_run_equals_single_context(mesh, nparts, precision, tol):
     one.close()
 
 
+def test_partitioned_tw_with_rayleigh_damping():
+    """Tchamwa-Wielgosz with Rayleigh alpha damping: the damped element
+    kernel reads nodal velocities, which every part must hold identically
+    at the shared nodes."""
+    import dataclasses
+    bar = dataclasses.replace(P.bar_40x4x4(nsteps=400), dampi=np.array([[2.0e5, 0.0]]))
+    one = sma.ExplicitSolid(bar, precision="fp64", scheme="tw", phitw=1.033)
+    one.step(200)
+    ps = PT.PartitionedSolid(bar, nparts=3, precision="fp64", scheme="tw", phitw=1.033)
+    ps.step(200)
+    for field in ("displ", "veloc"):
+        ref, got = one.get(field), ps.get(field)
+        assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max(), field
+
+
 def _free_port():
     import socket
     s = socket.socket()
