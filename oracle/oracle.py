@@ -46,6 +46,56 @@ def lib():
     return _lib
 
 
+COUNT_PATH = os.path.join(HERE, "liboracle_count.so")
+OPS = ("add", "mul", "div", "cmp", "sqrt", "log", "pow")
+_count_lib = None
+
+
+def count_lib():
+    """The oracle on a counting number type (liboracle_count.so)."""
+    global _count_lib
+    if _count_lib is None:
+        if not os.path.exists(COUNT_PATH):
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        L = C.CDLL(COUNT_PATH)
+        L.orc_count_law160.restype = C.c_int
+        L.orc_count_law160.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_double,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+        L.orc_count_element.restype = C.c_int
+        L.orc_count_element.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.c_double, C.c_double, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+        _count_lib = L
+    return _count_lib
+
+
+def count_law160(props, F, sdv, tmp=0.0, e_mart=0.0):
+    """Operations of one compute_kirchoff_stress call (F column-major, 9):
+    ({op: count}, sdv_new, nr_flag)."""
+    p = np.ascontiguousarray(props, dtype=np.float64).reshape(18)
+    f = np.ascontiguousarray(F, dtype=np.float64).reshape(9)
+    sv = np.array(sdv, dtype=np.float64)
+    ops = np.zeros(len(OPS), np.uint64)
+    fl = count_lib().orc_count_law160(_ptr(p, C.c_double), float(e_mart), _ptr(f, C.c_double), float(tmp),
+                                      _ptr(sv, C.c_double), _ptr(ops, C.c_uint64))
+    return dict(zip(OPS, (int(x) for x in ops))), sv, fl
+
+
+def count_element(elcod, eldis, props, densi, sdv_old, e_mart=0.0):
+    """Operations of one HEX08 element of the explicit element loop
+    (elcod, eldis (3, 8) column-major as 24; sdv_old (8, 3)):
+    ({op: count}, Gauss points that ran the return map)."""
+    c = np.ascontiguousarray(elcod, dtype=np.float64).reshape(24)
+    u = np.ascontiguousarray(eldis, dtype=np.float64).reshape(24)
+    p = np.ascontiguousarray(props, dtype=np.float64).reshape(18)
+    so = np.ascontiguousarray(sdv_old, dtype=np.float64).reshape(24)
+    ops = np.zeros(len(OPS), np.uint64)
+    nr = C.c_int(0)
+    count_lib().orc_count_element(_ptr(c, C.c_double), _ptr(u, C.c_double), _ptr(p, C.c_double), float(e_mart),
+                                  float(densi), _ptr(so, C.c_double), _ptr(ops, C.c_uint64), C.byref(nr))
+    return dict(zip(OPS, (int(x) for x in ops))), nr.value
+
+
 def _ptr(a, ctype):
     if a is None:
         return None
