@@ -107,7 +107,9 @@ def test_law_frame_indifference(precision, tol):
     and turns with a rotation of the reference configuration
     (S(F Q) = Q^T S(F) Q), with the same state update.  A rotation changes
     rounding, so a point sitting on a transformation threshold may switch
-    branch; such points (same flags required for 99 %) are left out."""
+    branch; such points (same flags required for 99 %) are left out.  The
+    FP32 form's absolute stress error under a rotation is ~E eps32 |F - I|
+    whatever the strain, so errors are taken relative to max(|S|, 1e-3 E)."""
     F, sdv = random_gauss_points(3000, seed=9)
     rng = np.random.default_rng(19)
     R = np.stack([rotation(rng) for _ in range(len(F))])
@@ -117,7 +119,7 @@ def test_law_frame_indifference(precision, tol):
     SQ, sQ, flQ = (x.cpu().numpy() for x in sma.eval_sld_stress_model_160(NITI, F @ Q, sdv, precision=precision))
     same = (fl == flR) & (fl == flQ)
     assert same.mean() >= 0.99
-    scale = np.abs(S).reshape(len(F), -1).max(axis=1)[same]
+    scale = np.maximum(np.abs(S).reshape(len(F), -1).max(axis=1), 1e-3 * NITI[0])[same]
     errR = np.abs(SR - S).reshape(len(F), -1).max(axis=1)[same] / scale
     SQ_back = np.einsum("gki,gkl,glj->gij", Q, S, Q)                # Q^T S Q
     errQ = np.abs(SQ - SQ_back).reshape(len(F), -1).max(axis=1)[same] / scale
