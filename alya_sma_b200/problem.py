@@ -337,7 +337,7 @@ def bar_40x4x4(nsteps=4000, seed=0, ref_equivalent=False, scale=1):
                    info=dict(mesh=f"{40*scale}x{4*scale}x{4*scale}", ref_equivalent=ref_equivalent))
 
 
-def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0)):
+def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0), layers=None):
     """NiTi cylinder r = 5 mm, L = 50 mm, HEX08 O-grid: a 32x32 core block and
     four 32x24 ring blocks per cross-section (4,096 cells), 488 layers
     (1,998,848 elements at div=1; every count divided by div).  Interior nodes
@@ -347,9 +347,14 @@ def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0)
     t_range[0] at x = 0 to t_range[1] at x = L; the transformation stresses
     shift by 6.5 MPa/K above 300 K (extension: the reference law has no
     temperature).  x = 0 clamped; the x = L face is pushed to -3 % axial strain
-    and released with smooth steps over nsteps steps of dt = 0.5 dt_crit."""
+    and released with smooth steps over nsteps steps of dt = 0.5 dt_crit.
+    layers: that many axial element layers instead, the length shortened so
+    the elements keep their size (a smaller case of the same mesh)."""
     nc, nr, nx = max(2, 32 // div), max(1, 24 // div), max(2, 488 // div)
-    coord, lnods = ogrid_cylinder(5.0, 50.0, nc, nr, nx, jitter=0.1, seed=seed)
+    length = 50.0
+    if layers:
+        length, nx = 50.0 * layers / nx, int(layers)
+    coord, lnods = ogrid_cylinder(5.0, length, nc, nr, nx, jitter=0.1, seed=seed)
     ne, npo = lnods.shape[0], coord.shape[0]
     rng = np.random.default_rng(seed + 1)
     base = nitinol_props(**NITI, C_AS=6.5 * SQRT_2_3, C_SA=6.5 * SQRT_2_3, T_ref=300.0)
@@ -364,18 +369,18 @@ def cylinder_2m(nsteps=10000, seed=0, div=1, spread=0.10, t_range=(300.0, 320.0)
     e_mart = NITI_E_MART * f[:, 6]
     densi = np.full(ne, NITI_DENSITY)
     xc = coord[lnods].mean(axis=1)[:, 0]
-    tempe = t_range[0] + (t_range[1] - t_range[0]) * xc / 50.0
+    tempe = t_range[0] + (t_range[1] - t_range[0]) * xc / length
     fixno = np.zeros((npo, 3), np.int32)
     bcfun = np.full(npo, -1, np.int32)
     x0 = face_nodes(coord, 0, 0.0)
-    xl = face_nodes(coord, 0, 50.0)
+    xl = face_nodes(coord, 0, length)
     fixno[x0] = 1
     fixno[xl, 0] = 1
     bcfun[xl] = 0
     lmate = np.arange(ne, dtype=np.int32)
     # E_M (at most 44 GPa here) stays below E_A (at least 54 GPa): E_A sets c
     dt = 0.5 * critical_dt(coord, lnods, props, densi, lmate)
-    tab = smooth_cycle_table(nsteps * dt, -0.03 * 50.0)
+    tab = smooth_cycle_table(nsteps * dt, -0.03 * length)
     return Problem(coord=coord, lnods=lnods, props=props, e_mart=e_mart, densi=densi,
                    fixno=fixno, bcfun=bcfun, fun_npts=np.array([3], np.int32),
                    fun_smooth=np.array([1], np.int32), fun_tab=tab, lmate=lmate, tempe=tempe,

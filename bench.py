@@ -1,13 +1,20 @@
 """Benchmark: Gauss-point updates/s of the explicit SMA (law 160) step.
 
-Workload (one GPU): NiTi cantilever 400x40x40 mm, HEX08 400x40x40 elements
-(640,000 elements, 674,081 nodes, 5.12 M Gauss points), jittered interior
-nodes, clamped root, axial tip traction cycled to 1.5x the forward-finish
-stress; central difference at dt = 0.5 dt_crit.  A step is one pass of the
-explicit scheme over the whole mesh (element loop + nodal update, BCs and
-time advanced on the device).  `value` times the FP32 precision form
-(FP32 kinematics and constitutive update, FP64 return map, force
-accumulation and integration); the plain FP64 form is timed beside it.
+Workload (one GPU): NiTi cylinder r = 5 mm, L = 50 mm, HEX08 O-grid of
+1,998,848 elements (2,034,729 nodes, 16.0 M Gauss points), interior nodes
+jittered U(-0.1,0.1)h, a material per element (E_A, E_M, eps_L and the four
+transformation stresses sampled +-10 % from a seed), temperature 300-320 K
+shifting the transformation stresses by 6.5 MPa/K, x = 0 clamped, x = L
+pushed to -3 % axial strain and released with smooth steps; central
+difference at dt = 0.5 dt_crit, prestrained 1 % so the return map is live.
+A step is one pass of the explicit scheme over the whole mesh (element loop
++ nodal update, BCs and time advanced on the device).  `value` times the
+FP32 precision form (FP32 kinematics and constitutive update, FP64 return
+map, force accumulation and integration); the plain FP64 form runs the same
+steps from the same start beside it, and `error_vs_fp64` compares the two
+at the end of the timed window (Gauss-point stress, displacement, martensite
+fraction, reaction on the pushed face).  --workload cantilever (640 k
+elements, tip traction) and ensemble (256 specimens) select the others.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp64] [--scatter atomic|color]
@@ -74,9 +81,15 @@ def parse():
     ap.add_argument("--div", type=int, default=1, help="coarsen the mesh (tests only)")
     ap.add_argument("--prestrain", type=float, default=0.01,
                     help="initial axial strain (both arms): 1%% is just past the AS start")
-    ap.add_argument("--workload", default="cantilever", choices=list(WORKLOADS),
-                    help="cantilever 400x40x40 (default), cylinder (2.0M-element O-grid, per-element "
-                         "materials, temperature field) or ensemble (256 specimens)")
+    ap.add_argument("--workload", default="cylinder", choices=list(WORKLOADS),
+                    help="cylinder (default: 2.0M-element O-grid, per-element materials, temperature "
+                         "field), cantilever 400x40x40 or ensemble (256 specimens)")
+    ap.add_argument("--layers", type=int, default=0,
+                    help="cylinder only: axial element layers (0: the full 488); a shorter cylinder "
+                         "is the profiling case of the same kernel")
+    ap.add_argument("--write-profile", metavar="CSV", default=None,
+                    help="turn `ncu -i <rep> --page raw --csv` output into the machine-read profile "
+                         "summary of this precision/workload (profiles/k_element_<prec>_<workload>.json)")
     ap.add_argument("--block", type=int, default=0, help="threads per element block (0: library default)")
     ap.add_argument("--autotune", action="store_true", help="pick block and scatter by timing candidates")
     ap.add_argument("--partition", action="store_true",
@@ -152,54 +165,122 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_summary(precision, workload, div):
-    """The committed ncu summary of the element kernel on this exact workload
-    (profiles/k_element_<precision>_<workload>.md), or None: a figure taken on
-    one mesh says nothing about a launch on another."""
-    if div != 1:
-        return None
-    return os.path.join(ROOT, "profiles", f"k_element_{precision}_{workload}.md")
+KERNEL_SOURCES = ("alya_sma_b200/csrc/sma_capi.cu", "alya_sma_b200/csrc/sma_kernels.cuh",
+                  "alya_sma_b200/csrc/sma_law.cuh", "alya_sma_b200/csrc/sma_surrogate.cuh",
+                  "alya_sma_b200/build.py")
 
 
-def profiled_traffic(path):
-    """DRAM bytes per element-kernel launch from an ncu summary
-    (line 'dram_bytes_per_launch: N')."""
-    if path is None:
-        return None
+def kernel_source_hash():
+    """Hash of the sources the element kernel is compiled from: a profile
+    taken on another build of the kernel says nothing about this one."""
+    import hashlib
+    h = hashlib.sha256()
+    for rel in KERNEL_SOURCES:
+        path = os.path.join(ROOT, rel)
+        if os.path.exists(path):
+            with open(path, "rb") as fh:
+                h.update(rel.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
+def profile_json(precision, workload):
+    return os.path.join(ROOT, "profiles", f"k_element_{precision}_{workload}.json")
+
+
+_UNITS = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12,
+          "KB": 1e3, "MB": 1e6, "GB": 1e9, "inst": 1.0, "Kinst": 1e3, "Minst": 1e6, "Ginst": 1e9,
+          "ns": 1e-9, "us": 1e-6, "usecond": 1e-6, "msecond": 1e-3, "nsecond": 1e-9, "ms": 1e-3,
+          "": 1.0, "warp": 1.0}
+
+
+def write_profile(csv_path, precision, workload, nelem, note=""):
+    """Machine-read summary of one ncu capture (`ncu -i rep --page raw --csv`)
+    of the element kernel: DRAM bytes and warp instructions per launch and
+    the number of elements the captured launch processed, stamped with the
+    hash of the kernel sources; written to profiles/ as JSON."""
+    import csv
+    with open(csv_path, newline="") as fh:
+        rows = list(csv.reader(fh))
+    head = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    names, units = rows[head], rows[head + 1]
+    col = {n: i for i, n in enumerate(names)}
+
+    def val(r, metric):
+        if metric not in col:
+            return None
+        raw = r[col[metric]].replace(",", "")
+        try:
+            return float(raw) * _UNITS.get(units[col[metric]].strip(), 1.0)
+        except ValueError:
+            return None
+
+    launches = [r for r in rows[head + 2:] if len(r) == len(names) and "k_element" in r[col["Kernel Name"]]]
+    if not launches:
+        raise SystemExit(f"no k_element launch in {csv_path}")
+    n = len(launches)
+    mean = lambda m: (sum(val(r, m) or 0.0 for r in launches) / n) if all(val(r, m) is not None for r in launches) else None
+    rd, wr = mean("dram__bytes_read.sum"), mean("dram__bytes_write.sum")
+    out = {"kernel": launches[0][col["Kernel Name"]], "precision": precision, "workload": workload,
+           "elements_per_launch": int(nelem), "launches_captured": n,
+           "dram_bytes_per_launch": (rd + wr) if rd is not None and wr is not None else None,
+           "dram_read_bytes_per_launch": rd, "dram_write_bytes_per_launch": wr,
+           "warp_inst_per_launch": mean("smsp__inst_executed.sum"),
+           "duration_s_under_ncu": mean("gpu__time_duration.sum"),
+           "registers_per_thread": mean("launch__registers_per_thread"),
+           "kernel_source_hash": kernel_source_hash(), "note": note}
+    path = profile_json(precision, workload)
+    with open(path, "w") as fh:
+        json.dump(out, fh, indent=1)
+        fh.write("\n")
+    print(path)
+    return out
+
+
+def load_profile(precision, workload, nelem):
+    """The machine-written ncu summary of the element kernel for this
+    precision and workload, scaled from the captured launch's element count
+    to `nelem` (traffic and instructions grow with the elements processed),
+    or None when there is none or it was taken on other kernel sources."""
     try:
-        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-        return float(m.group(1)) if m else None
-    except OSError:
+        with open(profile_json(precision, workload)) as fh:
+            p = json.load(fh)
+    except (OSError, ValueError):
         return None
+    if p.get("kernel_source_hash") != kernel_source_hash():
+        return None
+    k = nelem / float(p["elements_per_launch"])
+    return {"traffic": None if p.get("dram_bytes_per_launch") is None else p["dram_bytes_per_launch"] * k,
+            "warp_inst": None if p.get("warp_inst_per_launch") is None else p["warp_inst_per_launch"] * k,
+            "scaled_from_elements": p["elements_per_launch"], "sms": 148}
 
 
-def profiled_issue(path):
-    """Warp instructions per element-kernel launch from the same ncu summary
-    (line 'warp_inst_per_launch: N'); the B200 has 148 SMs."""
-    if path is None:
-        return None
-    try:
-        m = re.search(r"warp_inst_per_launch:\s*([0-9.eE+]+)", open(path).read())
-        return {"warp_inst": float(m.group(1)), "sms": 148} if m else None
-    except OSError:
-        return None
+def per_element_values(prob):
+    """Material values the element kernel needs per element: the seven the
+    cylinder and the ensemble sample (E_A, E_M, eL, four transformation
+    stresses) plus the temperature with per-element materials; the
+    temperature alone with one material and a temperature field."""
+    if len(prob.props) > 1:
+        return 8
+    return 1 if prob.tempe is not None else 0
 
 
 def algorithmic_bytes(prob, precision):
     """Minimum HBM traffic of one element-kernel launch: connectivity, state
-    read + write, one read of coordinates and displacements and one
+    read + write, the per-element material values and temperature (in the
+    precision's word), one read of coordinates and displacements and one
     read-modify-write of the residual per node."""
     s = 4 if precision == "fp32" else 8
-    return prob.nelem * (32 + 2 * 8 * 3 * s) + prob.npoin * (24 + 24 + 48)
+    return prob.nelem * (32 + 2 * 8 * 3 * s + per_element_values(prob) * s) + prob.npoin * (24 + 24 + 48)
 
 
-def build_problem(workload, div, rank=0, world=1):
+def build_problem(workload, div, rank=0, world=1, layers=0):
     """The workload's mesh on this rank.  The ensemble shards its specimens
     across ranks (largest first onto the least loaded rank); the other
-    workloads run one replica per rank."""
+    workloads run one replica per rank.  layers > 0 shortens the cylinder to
+    that many axial element layers (same cross-section and element size)."""
     from alya_sma_b200 import problem as P
     if workload == "cylinder":
-        return P.cylinder_2m(nsteps=10000, div=div)
+        return P.cylinder_2m(nsteps=10000, div=div, layers=layers or None)
     if workload == "ensemble":
         nspec = max(2, 256 // div)
         if world > 1:
@@ -210,13 +291,45 @@ def build_problem(workload, div, rank=0, world=1):
     return P.cantilever_400x40x40(nsteps=20000, div=div)
 
 
+def compare_forms(prob, s32, s64, nsteps):
+    """Error of the FP32 precision form against the plain FP64 form after the
+    same `nsteps` steps from the same start: Gauss-point Cauchy stress
+    (relative to the largest |sigma| of the FP64 run), nodal displacement
+    (relative to the largest |u|), the mean axial displacement of the far
+    face x = max (the cantilever's tip), the axial reaction on the far face
+    where it is held (the cylinder's pushed face), and the largest martensite
+    fraction difference.  The north star bounds the stress at 1e-3 and the
+    tip displacement at 1e-4."""
+    g32 = s32.postprocess(gp_sigma=True)["gp_sigma"]
+    g64 = s64.postprocess(gp_sigma=True)["gp_sigma"]
+    smax = float(np.abs(g64).max())
+    stress = float(np.abs(g32 - g64).max()) / smax
+    del g32, g64
+    u32, u64 = s32.get("displ"), s64.get("displ")
+    X = prob.coord
+    far = np.isclose(X[:, 0], X[:, 0].max())
+    tip32, tip64 = u32[far, 0].mean(), u64[far, 0].mean()
+    out = {"steps": int(nsteps), "stress_rel": stress, "max_abs_stress_mpa": smax,
+           "displacement_rel": float(np.abs(u32 - u64).max() / np.abs(u64).max()),
+           "far_face_ux_rel": float(abs(tip32 - tip64) / max(abs(tip64), 1e-300)),
+           "xS_max_abs": float(np.abs(s32.state[:, 1, :, 0] - s64.state[:, 1, :, 0]).max()),
+           "bounds": {"stress_rel": 1e-3, "tip_displacement_rel": 1e-4},
+           "what": "FP32 form vs plain FP64 form after the same steps from the same start: Gauss-point "
+                   "Cauchy stress, nodal displacement, far-face axial displacement, martensite fraction"}
+    held = far & (prob.fixno[:, 0] == 1)
+    if held.any():
+        r32, r64 = s32.get("rhsid")[held, 0].sum(), s64.get("rhsid")[held, 0].sum()
+        out["far_face_reaction_rel"] = float(abs(r32 - r64) / max(abs(r64), 1e-300))
+    return out
+
+
 def cpu_baseline(prob, u0, budget_s=15.0, max_steps=50):
     """The oracle's central-difference step (colour-parallel element loop,
-    OpenMP over all host threads) on the full mesh, as many steps as fit in
-    about budget_s seconds."""
+    OpenMP over all host threads, compiled with -march=native on this host)
+    on the full mesh, as many steps as fit in about budget_s seconds."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    o = O.Problem(prob, nthreads=threads)
+    o = O.Problem(prob, nthreads=threads, native=True)
     o.displ[:] = u0
     o.run(prob.dtime, 1)                      # warm-up (page-in, thread pool)
     steps, t0 = 0, time.perf_counter()
@@ -228,7 +341,20 @@ def cpu_baseline(prob, u0, budget_s=15.0, max_steps=50):
     dt = time.perf_counter() - t0
     return {"value": prob.nelem * 8 * steps / dt, "unit": "GP-updates/s", "cores": threads,
             "kind": "port", "sample": f"{steps} central-difference steps of the full "
-                                      f"{prob.nelem}-element mesh ({dt:.1f} s)"}
+                                      f"{prob.nelem}-element mesh ({dt:.1f} s), "
+                                      + ("-O3 -march=native" if o.native else "-O3 -march=x86-64-v3")
+                                      + f" -fopenmp on {cpu_model()}"}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
 
 
 def run_reference(args):
@@ -236,7 +362,7 @@ def run_reference(args):
     if world > 1 and rank != 0:
         return 0
     from alya_sma_b200 import problem as P
-    prob = build_problem(args.workload, args.div)
+    prob = build_problem(args.workload, args.div, layers=args.layers)
     u0 = P.prestrain(prob, args.prestrain)
     base = cpu_baseline(prob, u0, budget_s=15.0, max_steps=max(2, args.steps))
     line = {"impl": "reference", "metric": "Gauss-point updates/s (explicit SMA step)",
@@ -267,7 +393,7 @@ def run_partitioned(args, rank, world, local):
     from alya_sma_b200 import dist as D
     from alya_sma_b200 import partition as PT
     from alya_sma_b200 import problem as P
-    prob = build_problem(args.workload, args.div)
+    prob = build_problem(args.workload, args.div, layers=args.layers)
     group = torch.distributed.group.WORLD if world > 1 else None
     ps = PT.PartitionedSolid(prob, nparts=1, precision=args.precision, scatter=args.scatter, device=local,
                              group=group, block=args.block)
@@ -318,10 +444,11 @@ def run_partitioned(args, rank, world, local):
     alg = algorithmic_bytes(q, args.precision)
     peak, peak_kind = measured_peaks()
     achieved = alg / (el_ms / 1e3) / 1e9
-    summary = profile_summary(args.precision, args.workload, args.div) if world == 1 else None
+    prof = load_profile(args.precision, args.workload, q.nelem) if (world == 1 and args.div == 1
+                                                                       and not args.layers) else None
     roofline = {"bound": "hbm", "kernel": "k_element", "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": profiled_traffic(summary), "algorithmic_bytes_per_launch": alg,
+                "traffic": prof["traffic"] if prof else None, "algorithmic_bytes_per_launch": alg,
                 "launch_ms": round(el_ms, 4), "exchange_ms": round(ex_ms, 4), "nodal_launch_ms": round(nd_ms, 4),
                 "window": "rank 0's part, per-step CUDA events on its stream over a second K-step window",
                 "note": "compute-bound kernel: the FP32/FP64 pipes, not HBM, bind it"}
@@ -349,6 +476,12 @@ def run_partitioned(args, rank, world, local):
 
 def main():
     args = parse()
+    if args.write_profile:
+        prob = build_problem(args.workload, args.div, layers=args.layers)
+        note = (f"captured on the {prob.nelem}-element case (--layers {args.layers}); bench.py scales "
+                "traffic and instructions to the bench mesh by element count") if args.layers else ""
+        write_profile(args.write_profile, args.precision, args.workload, prob.nelem, note)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -362,7 +495,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     if args.partition:
         return run_partitioned(args, rank, world, local)
-    prob = build_problem(args.workload, args.div, rank, world)
+    prob = build_problem(args.workload, args.div, rank, world, layers=args.layers)
     nelem, ngp = prob.nelem, prob.nelem * 8
     sharded = args.workload == "ensemble" and world > 1       # strong scaling: fixed total work
 
@@ -437,45 +570,49 @@ def main():
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes(prob, args.precision)
     achieved = alg / (el_ms / 1e3) / 1e9
-    summary = profile_summary(args.precision, args.workload, args.div)
-    traffic = profiled_traffic(summary)
+    prof = load_profile(args.precision, args.workload, nelem) if (args.div == 1 and not args.layers) else None
     roofline = {"bound": "hbm", "kernel": "k_element", "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic,
-                "algorithmic_bytes_per_launch": alg, "launch_ms": round(el_ms, 4),
-                "nodal_launch_ms": round(nd_ms, 4),
+                "frac": round(achieved / peak, 4), "traffic": prof["traffic"] if prof else None,
+                "algorithmic_bytes_per_launch": alg,
+                "algorithmic_bytes_per_gauss_point": round(alg / ngp, 1),
+                "launch_ms": round(el_ms, 4), "nodal_launch_ms": round(nd_ms, 4),
                 "window": "the K timed steps replayed from a checkpoint of their start, "
                           "CUDA events around each launch on the library stream",
+                "profile": (f"profiles/k_element_{args.precision}_{args.workload}.json, scaled from "
+                            f"{prof['scaled_from_elements']} elements" if prof else
+                            "no ncu summary of this kernel build and workload: traffic not reported"),
                 "note": "compute-bound kernel: the FP32/FP64 pipes, not HBM, bind it"}
-    issue = profiled_issue(summary)
-    if issue:
+    if prof and prof["warp_inst"]:
         # instruction-issue roofline: warp instructions per launch (ncu) over
         # the measured launch time, against 4 issue slots per SM per clock
-        rate = issue["warp_inst"] / (el_ms / 1e3)
-        peak_i = 4 * issue["sms"] * ck.get("sm_mhz", 1965.0) * 1e6
-        roofline["issue"] = {"warp_inst_per_launch": issue["warp_inst"],
+        rate = prof["warp_inst"] / (el_ms / 1e3)
+        peak_i = 4 * prof["sms"] * ((ck or {}).get("sm_mhz") or 1965.0) * 1e6
+        roofline["issue"] = {"warp_inst_per_launch": round(prof["warp_inst"]),
                              "achieved_ginst_s": round(rate / 1e9, 1),
                              "peak_ginst_s": round(peak_i / 1e9, 1),
                              "frac": round(rate / peak_i, 4)}
 
     extras = {}
-    if not args.no_extras and rank == 0:
-        # plain FP64 form on the same mesh
-        if args.precision != "fp64":
-            s64 = sma.ExplicitSolid(prob, precision="fp64", scatter=args.scatter, device=local)
-            s64.set("displ", u0)
-            s64.step(max(3, args.warmup))
-            st64 = torch.cuda.ExternalStream(s64.stream)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            k64 = max(20, args.steps // 4)
-            a.record(st64)
-            s64.step(k64)
-            b.record(st64)
-            b.synchronize()
-            v64 = ngp * k64 / (a.elapsed_time(b) / 1e3)
-            extras["plain_fp64"] = {"value": v64, "unit": "GP-updates/s", "steps": k64}
-            extras["speedup_vs_plain_fp64"] = round(value / world / v64, 3)
-            s64.close()
+    if not args.no_extras and rank == 0 and args.precision != "fp64":
+        # the plain FP64 form: the same steps from the same start, its K
+        # steps timed like the FP32 window; then both forms compared
+        wsteps = max(3, args.warmup)
+        s64 = sma.ExplicitSolid(prob, precision="fp64", scatter=args.scatter, device=local)
+        s64.set("displ", u0)
+        s64.step(wsteps)
+        st64 = torch.cuda.ExternalStream(s64.stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st64)
+        s64.step(args.steps)
+        b.record(st64)
+        b.synchronize()
+        v64 = ngp * args.steps / (a.elapsed_time(b) / 1e3)
+        extras["plain_fp64"] = {"value": v64, "unit": "GP-updates/s", "steps": args.steps,
+                                "ms_per_step": a.elapsed_time(b) / args.steps}
+        extras["speedup_vs_plain_fp64"] = round(value / world / v64, 3)
+        extras["error_vs_fp64"] = compare_forms(prob, solid, s64, wsteps + args.steps)
+        s64.close()
     if not args.no_extras:
         # e2e on every rank: the element-loop C-ABI call with pinned host
         # buffers, host copies inside the timed region; the job's Gauss points

@@ -46,6 +46,27 @@ def lib():
     return _lib
 
 
+NATIVE_PATH = os.path.join(HERE, "liboracle_native.so")
+_native_lib = None
+
+
+def native_lib():
+    """The same oracle compiled with -march=native for the machine it runs on
+    (the timed CPU baseline): built there by `make native`, since a library
+    tuned for one host's instruction set may not run on another's.  Falls
+    back to the portable liboracle.so when the build fails; returns
+    (library, True if native)."""
+    global _native_lib
+    if _native_lib is None:
+        try:
+            subprocess.run(["make", "-s", "-B", "-C", HERE, "native"], check=True,
+                           capture_output=True, timeout=300)
+            _native_lib = (C.CDLL(NATIVE_PATH), True)
+        except (OSError, subprocess.SubprocessError):
+            _native_lib = (lib(), False)
+    return _native_lib
+
+
 COUNT_PATH = os.path.join(HERE, "liboracle_count.so")
 OPS = ("add", "mul", "div", "cmp", "sqrt", "log", "pow")
 _count_lib = None
@@ -215,8 +236,9 @@ class Problem:
     Built from the package's mesh/problem description (duck-typed: any object
     with the attributes read below works)."""
 
-    def __init__(self, p, dtype=np.float64, nthreads=None):
+    def __init__(self, p, dtype=np.float64, nthreads=None, native=False):
         npt, ct, sfx = _f(dtype)
+        self._lib, self.native = native_lib() if native else (lib(), False)
         self.dtype, self.ct, self.sfx = npt, ct, sfx
         self.nthreads = nthreads or os.cpu_count() or 1
         self.lnods = np.ascontiguousarray(p.lnods, dtype=np.int32)
@@ -262,7 +284,7 @@ class Problem:
         out = {k: np.zeros(n3, self.dtype) for k in ("rhsid", "finte", "fexte", "frxid")}
         out["vmass"] = np.zeros(self.npoin, self.dtype)
         dmin = np.zeros(1, self.dtype)
-        fn = getattr(lib(), "orc_assemble" + self.sfx)
+        fn = getattr(self._lib, "orc_assemble" + self.sfx)
         fn(self.nelem, self.npoin, _ptr(self.lnods, C.c_int32), _ptr(self.coord, ct), _ptr(d, ct),
            _ptr(self.lmate, C.c_int32), _ptr(self.props, ct), _ptr(self.e_mart, ct),
            _ptr(self.densi, ct), _ptr(self.tempe, ct), None, _ptr(self.fext, ct),
@@ -289,7 +311,7 @@ class Problem:
         gf = {k: np.zeros((self.nelem, 8, 3, 3), self.dtype) for k in ("gpgdi", "gppio")} if gauss else {}
         gdet = np.zeros((self.nelem, 8), self.dtype) if gauss else None
         vol = np.zeros(2, self.dtype) if gauss else None
-        fn = getattr(lib(), "orc_postprocess" + self.sfx)
+        fn = getattr(self._lib, "orc_postprocess" + self.sfx)
         fn.argtypes = None
         rc = fn(self.nelem, self.npoin, _ptr(self.lnods, C.c_int32), _ptr(self.coord, ct),
                 _ptr(d, ct), _ptr(self.lmate, C.c_int32), _ptr(self.props, ct),
@@ -321,7 +343,7 @@ class Problem:
         if wit.size and (wit.min() < 0 or wit.max() >= 3 * self.npoin):
             raise ValueError("oracle witnesses are displacement dofs in [0, 3*npoin)")
         hist = np.zeros((nsteps, max(1, wit.size)), self.dtype)
-        fn = getattr(lib(), "orc_run_cd" + self.sfx)
+        fn = getattr(self._lib, "orc_run_cd" + self.sfx)
         fn.argtypes = None
         fn(self.nelem, self.npoin, _ptr(self.lnods, C.c_int32), _ptr(self.coord, ct),
            _ptr(self.lmate, C.c_int32), _ptr(self.props, ct), _ptr(self.e_mart, ct),
@@ -335,3 +357,36 @@ class Problem:
            _ptr(hist, ct), _ptr(self.counters, C.c_int32), 1 if scheme == "tw" else 0, ct(phi),
            _ptr(self.dampi, ct))
         return hist[:, : wit.size]
+
+
+# -- learned surrogate's network (FP64 restatement, sma_mlp.c) --------------
+MLP_NIN, MLP_NOUT = 14, 13
+
+
+def mlp_nparam():
+    return int(lib().orc_mlp_nparam())
+
+
+def mlp_forward(params, stats, x):
+    """Raw outputs (n, 13) of the network on raw inputs x (n, 14)."""
+    p = np.ascontiguousarray(params, np.float64)
+    s = np.ascontiguousarray(stats, np.float64)
+    xx = np.ascontiguousarray(x, np.float64).reshape(-1, MLP_NIN)
+    y = np.zeros((xx.shape[0], MLP_NOUT))
+    lib().orc_mlp_forward(_ptr(p, C.c_double), _ptr(s, C.c_double), C.c_int64(xx.shape[0]),
+                          _ptr(xx, C.c_double), _ptr(y, C.c_double))
+    return y
+
+
+def mlp_loss_grad(params, stats, x, y, grad=True):
+    """(loss, gradient) of the normalised mean squared error of the batch."""
+    p = np.ascontiguousarray(params, np.float64)
+    s = np.ascontiguousarray(stats, np.float64)
+    xx = np.ascontiguousarray(x, np.float64).reshape(-1, MLP_NIN)
+    yy = np.ascontiguousarray(y, np.float64).reshape(-1, MLP_NOUT)
+    g = np.zeros(p.size) if grad else None
+    fn = lib().orc_mlp_loss_grad
+    fn.restype = C.c_double
+    loss = fn(_ptr(p, C.c_double), _ptr(s, C.c_double), C.c_int64(xx.shape[0]), _ptr(xx, C.c_double),
+              _ptr(yy, C.c_double), _ptr(g, C.c_double) if grad else None)
+    return float(loss), g

@@ -134,7 +134,7 @@ void FN(orc_dsyevq3)(const REAL A[9], REAL Q[9], REAL w[3], int* fail)
   }
 }
 
-/* eigsrt.f90:275-294: selection sort, largest eigenvalue first (ties move). */
+/* eigsrt.f90:19-48: selection sort, largest eigenvalue first (ties move). */
 void FN(orc_eigsrt)(REAL d[3], REAL V[9])
 {
   for (int i = 0; i < 2; ++i) {
