@@ -59,7 +59,7 @@ class _Run(C.Structure):
 
 
 SCHEME = {"cd": 0, "tw": 1}
-VARIANT = {"auto": 0, "pipe": 1, "plain": 2}
+VARIANT = {"auto": 0, "pipe": 1, "plain": 2, "table": 3}
 
 
 class _Counters(C.Structure):
@@ -272,6 +272,8 @@ class ExplicitSolid:
         if reset:
             _check(lib().sma_reset_counters(self._ctx))
         out = {name: int(c.c[i]) for i, name in enumerate(COUNTERS)}
+        out["sur_fallback"] = int(c.c[5])                     # surrogate points sent to the plain law
+        out["sur_ood"] = int(c.c[7])                          # of those, out of the envelope
         out["gpdet_min"] = float(c.gpdet_min)                 # smallest det F <= 0, 0.0 if none
         out["ielem_min"] = int(c.ielem_min)                   # its element, -1 if none
         return out
@@ -299,6 +301,27 @@ class ExplicitSolid:
         n = C.c_int32()
         _check(lib().sma_get_witness(self._ctx, _p(out), C.byref(n)))
         return out[: n.value]
+
+    def set_surrogate(self, net, gate=3.0, xs_tol=1e-3, enable=True):
+        """The learned surrogate (alya_sma_b200.surrogate.Surrogate) in the
+        element loop of this FP32 context (sma_set_surrogate), or back to the
+        plain law with enable=False."""
+        L = lib()
+        L.sma_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32]
+        if not enable:
+            _check(L.sma_set_surrogate(self._ctx, None, None, 1.0, 0.0, 0))
+            return
+        w = np.ascontiguousarray(net.params(), dtype=np.float32)
+        st = net.stats_host
+        _check(L.sma_set_surrogate(self._ctx, w.ctypes.data, C.addressof(st), float(gate), float(xs_tol), 1))
+        self._sur_keep = (w, st)
+
+    def surrogate_status(self):
+        s = C.c_int32()
+        L = lib()
+        L.sma_surrogate_status.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+        _check(L.sma_surrogate_status(self._ctx, C.byref(s)))
+        return int(s.value)
 
     def critical_dt(self):
         d = C.c_double()

@@ -12,6 +12,7 @@
 
 #include "alya_sma.h"
 #include "sma_kernels.cuh"
+#include "sma_surrogate_elem.cuh"
 
 using namespace sma;
 
@@ -50,6 +51,11 @@ int32_t dalloc(P** p, size_t bytes) {
 }
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// per-element materials use compact records when a material is shared by at
+// most this many elements on average (more sharing: the material table,
+// which the caches hold)
+constexpr int COMPACT_MAX_SHARING = 4;
 
 // host restatement of sld_elmmat.f90:199-209 summed per node in element
 // order (deterministic); FP64 geometry as jacobi.f90:172-219
@@ -197,6 +203,11 @@ MatC make_mat(const double* pr, double e_mart, double densi) {
 
 }  // namespace
 
+// the error text of the other translation units of the library (not exported)
+extern "C" __attribute__((visibility("hidden"))) int32_t sma_set_error_(int32_t code, const char* msg) {
+  return fail(code, msg ? msg : "");
+}
+
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
@@ -233,6 +244,16 @@ struct sma_ctx {
   int8_t* d_bcfun = nullptr;
   MatC* d_mats = nullptr;
   MatC mat0;                               // material 0, passed by value when nmate == 1
+  void* d_matx = nullptr;                  // compact per-element records (T [nelem][MATX]) or null
+  bool compact = false;                    // element kernel reads d_matx instead of d_mats
+  // learned surrogate (FP32 form): weight image, statistics, eps_tr ping-pong
+  bool sur = false;
+  unsigned char* d_sur_img = nullptr;
+  sur::SurStats* d_sur_stats = nullptr;
+  float* d_etr[2] = {nullptr, nullptr};    // [6][sst] per state buffer
+  int* d_sur_ctr = nullptr;                // [0] tile counter, [1] status
+  float sur_gate = 3.0f, sur_xs_tol = 1e-3f;
+  int sur_grid = 0;
   void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
   int cur = 0;                             // state buffer holding TIME_N
   int last_in = -1;                        // state buffer the last element loop read (-1: none)
@@ -354,6 +375,7 @@ ElemArgs<T> elem_args(sma_ctx* c, int beg, int end, bool advance, bool stepping 
   a.beg = beg;
   a.end = end;
   a.mat0 = c->mat0;
+  a.matx = (const T*)c->d_matx;
   // one wave of the one-tile kernel: every SM's resident blocks of block / 8 elements
   a.pf_ahead = (c->variant == SMA_VARIANT_PIPE) ? 0 : (int64_t)c->nsm * c->resident * (c->block / 8);
   a.grav[0] = c->grav[0];
@@ -383,6 +405,11 @@ ElemKernel<T> elem_kernel(const sma_ctx* c) {
   const bool atomic = c->scatter != SMA_SCATTER_COLOR;
   const bool mats = c->d_lmate != nullptr;
   const int b = c->block;
+  if (c->compact) {                                              // one-tile, undamped
+    const bool narrow = b <= ELEM_NARROW_BLOCK;
+    if (atomic) return narrow ? k_element<T, true, true, false, true, true> : k_element<T, true, true, false, false, true>;
+    return narrow ? k_element<T, false, true, false, true, true> : k_element<T, false, true, false, false, true>;
+  }
   if (c->damp) {                                                 // one-tile kernel only
     if (atomic) return mats ? k_element<T, true, true, true> : k_element<T, true, false, true>;
     return mats ? k_element<T, false, true, true> : k_element<T, false, false, true>;
@@ -393,7 +420,7 @@ ElemKernel<T> elem_kernel(const sma_ctx* c) {
 
 template <typename T>
 size_t elem_smem(const sma_ctx* c) {
-  const bool mats = c->d_lmate != nullptr;
+  const bool mats = c->d_lmate != nullptr && !c->compact;
   return c->variant == SMA_VARIANT_PIPE ? element_pipe_smem_bytes<T>(c->block, mats)
                                         : element_smem_bytes<T>(c->block, mats);
 }
@@ -416,11 +443,42 @@ int32_t init_element_launch_t(sma_ctx* c) {
   return SMA_OK;
 }
 
+// the surrogate element kernel on elements [beg, end): persistent blocks,
+// tiles handed out by a counter cleared first (a memset node in graphs)
+int32_t launch_sur_range(sma_ctx* c, int beg, int end, bool advance, bool stepping) {
+  if (end <= beg) return SMA_OK;
+  ElemArgs<float> a = elem_args<float>(c, beg, end, advance, stepping);
+  sur::SurElemArgs s;
+  s.img = c->d_sur_img;
+  s.stats = c->d_sur_stats;
+  s.etr_old = c->d_etr[c->cur];
+  s.etr_new = c->d_etr[c->cur ^ 1];
+  s.tile_ctr = c->d_sur_ctr;
+  s.status = c->d_sur_ctr + 1;
+  s.gate = c->sur_gate;
+  s.xs_tol = c->sur_xs_tol;
+  CU(cudaMemsetAsync(c->d_sur_ctr, 0, sizeof(int), c->stream));
+  const int64_t ntiles = ceil_div(end - beg, sur::SUR_EPB);
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, c->sur_grid);
+  const size_t smem = sur::sur_elem_smem_bytes();
+  if (c->compact) sur::k_element_sur<true><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
+  else sur::k_element_sur<false><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
 template <typename T>
 int32_t launch_elements_t(sma_ctx* c, bool advance) {
   const int nrange = (int)c->cptr.size() - 1;
   const int epb = c->block / 8;
   if (c->resident == 0) return fail(SMA_ERR_STATE, "element launch not initialised");
+  if constexpr (sizeof(T) == 4) {
+    if (c->sur) {
+      c->last_in = c->cur;
+      return launch_sur_range(c, 0, c->nelem, advance, advance);
+    }
+  }
   c->last_in = c->cur;
   const ElemKernel<T> kern = elem_kernel<T>(c);
   const size_t smem = elem_smem<T>(c);
@@ -448,6 +506,8 @@ int32_t launch_elements(sma_ctx* c, bool advance) {
 template <typename T>
 int32_t launch_element_range_t(sma_ctx* c, int beg, int end) {
   if (end <= beg) return SMA_OK;
+  if constexpr (sizeof(T) == 4)
+    if (c->sur) return launch_sur_range(c, beg, end, false, false);
   const int epb = c->block / 8;
   ElemArgs<T> a = elem_args<T>(c, beg, end, false, false);
   const int64_t ntiles = ceil_div(end - beg, epb);
@@ -745,7 +805,8 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
   destroy_graphs(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->l2_window) cudaCtxResetPersistingL2Cache();   // release the lines this context pinned
-  void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_nodal,
+  void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_nodal, c->d_matx, c->d_sur_img, c->d_sur_stats,
+                  c->d_etr[0], c->d_etr[1], c->d_sur_ctr,
                   c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
@@ -843,10 +904,12 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   // elements, fixed step windows): the one-tile kernel in both precisions;
   // with the register caps of the element kernels the pipelined variant
   // spills and is 10-50 % slower
-  if (run->variant == SMA_VARIANT_AUTO)
+  if (run->variant < SMA_VARIANT_AUTO || run->variant > SMA_VARIANT_TABLE)
+    { sma_ctx_destroy(c); return fail(SMA_ERR_ARG, "variant must be one of SMA_VARIANT_*"); }
+  if (run->variant == SMA_VARIANT_AUTO || run->variant == SMA_VARIANT_TABLE)
     c->variant = SMA_VARIANT_PLAIN;
   else
-    c->variant = (run->variant == SMA_VARIANT_PLAIN) ? SMA_VARIANT_PLAIN : SMA_VARIANT_PIPE;
+    c->variant = run->variant;
   // default block, measured on B200 over fixed step windows: the one-tile
   // kernel at 32 threads (one warp, 4 elements) with one material (finer
   // scheduling at the same warps per SM, no block barrier: against 128,
@@ -916,6 +979,55 @@ int32_t sma_ctx_create(const sma_mesh_desc* mesh, const sma_material_desc* mat,
   TRY(dalloc(&c->d_mats, mats.size() * sizeof(MatC)));
   TRYCU(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(MatC), cudaMemcpyHostToDevice));
   c->mat0 = mats[0];
+  // Compact per-element records when the materials differ only in what the
+  // record holds (moduli, eL, thresholds; the temperature rides along) and
+  // are many: 64 bytes per element read into registers instead of the
+  // 176-byte material staged through shared memory behind a block barrier.
+  // Measured on B200: the 2.0 M-element cylinder (a material per element)
+  // -15 % FP32 / -6 % FP64 element time; the 256-specimen ensemble (256
+  // materials, a table the caches hold) +16 % FP32, so a few materials keep
+  // the table.  The one-tile undamped kernel reads them; SMA_VARIANT_TABLE
+  // keeps the table.
+  if (c->d_lmate && (int64_t)c->nmate * COMPACT_MAX_SHARING >= c->nelem && c->variant == SMA_VARIANT_PLAIN &&
+      !c->damp &&
+      run->variant != SMA_VARIANT_TABLE) {
+    bool shared = true;
+    for (const MatC& m : mats)
+      shared = shared && m.kK == c->mat0.kK && m.kG == c->mat0.kG && m.alfa == c->mat0.alfa &&
+               m.C_AS == c->mat0.C_AS && m.C_SA == c->mat0.C_SA && m.densi == c->mat0.densi &&
+               m.ray_a == c->mat0.ray_a;
+    if (shared) {
+      std::vector<double> rec((size_t)c->nelem * MATX);
+      for (int e = 0; e < c->nelem; ++e) {
+        const MatC& m = mats[mesh->lmate[c->perm[e]]];
+        double* r = rec.data() + (size_t)e * MATX;
+        r[MX_IEA] = m.iEA;
+        r[MX_IEM] = m.iEM;
+        r[MX_EL] = m.eL;
+        r[MX_RS_AS] = m.Rs_AS;
+        r[MX_RF_AS] = m.Rf_AS;
+        r[MX_RS_SA] = m.Rs_SA;
+        r[MX_RF_SA] = m.Rf_SA;
+        r[MX_TEMP] = mat->tempe ? mat->tempe[c->perm[e]] : 0.0;
+      }
+      if (c->prec == SMA_PREC_FP32) {
+        // offsets from material 0 (temperature: from the first element's)
+        c->mat0.T0 = rec[MX_TEMP];
+        const double base[MATX] = {c->mat0.iEA, c->mat0.iEM, c->mat0.eL, c->mat0.Rs_AS, c->mat0.Rf_AS,
+                                   c->mat0.Rs_SA, c->mat0.Rf_SA, c->mat0.T0};
+        std::vector<float> rf(rec.size());
+        for (size_t q = 0; q < rec.size(); ++q) rf[q] = (float)(rec[q] - base[q % MATX]);
+        TRY(dalloc(&c->d_matx, rf.size() * sizeof(float)));
+        TRYCU(cudaMemcpy(c->d_matx, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice));
+      } else {
+        TRY(dalloc(&c->d_matx, rec.size() * sizeof(double)));
+        TRYCU(cudaMemcpy(c->d_matx, rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+      }
+      c->compact = true;
+      // no block barrier: one-warp blocks, as with one material
+      if (!run->block) c->block = 32;
+    }
+  }
 
   // nodal arrays (SoA [3][npad])
   const size_t nb = 3 * (size_t)c->npad * sizeof(double);
@@ -1377,7 +1489,7 @@ int32_t sma_get_counters(sma_ctx* c, sma_counters* out) {
   unsigned long long h[NCNT];
   CU(cudaMemcpyAsync(h, c->d_cnt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k < CNT_DETMIN) ? (int64_t)h[k] : 0;
+  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k != CNT_DETMIN) ? (int64_t)h[k] : 0;
   // the smallest det F <= 0 seen and its element (caller's numbering)
   const unsigned long long dm = h[CNT_DETMIN];
   if (dm == ~0ull) {
@@ -1706,7 +1818,8 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   T* s_iterk = (T*)(base + NA_OFF_S0);
   T* s_timen = (T*)(base + NA_OFF_S1);
   const unsigned sgrid = (unsigned)ceil_div(8 * (int64_t)nelem, 256);
-  k_state_in<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
+  // the caller's slot TIME_N in, slot ITER_K out: the other slot is left as it is
+  k_state_in<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, nullptr, s_timen, nelem, sst);
   ElemArgs<T> a;
   std::memset(&a, 0, sizeof a);
   a.lnods = d_lnods;
@@ -1733,7 +1846,7 @@ int32_t noalloc_run(unsigned char* base, int32_t nelem, int32_t npoin, const int
   const int block = 32, epb = block / 8;
   const size_t smem = element_smem_bytes<T>(block, false);      // below the 48 KB default
   k_element<T, true, false, false, true><<<(unsigned)ceil_div(nelem, epb), block, smem, s>>>(a);
-  k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, s_timen, nelem, sst);
+  k_state_out<T><<<sgrid, 256, 0, s>>>(d_sdv, nullptr, s_iterk, nullptr, nelem, sst);
   CU(cudaGetLastError());
   return SMA_OK;
 }
@@ -1780,9 +1893,12 @@ extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int3
   CU(cudaMemcpyAsync(&bad, d_flag, sizeof bad, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   if (bad) return fail(SMA_ERR_ARG, "lnods holds node ids outside [0, npoin)");
-  // the scratch keeps the previous call's contents: clear what accumulates
+  // the scratch keeps the previous call's contents: clear what accumulates,
+  // and mark "no det F <= 0 seen" as the context does (all ones)
   CU(cudaMemsetAsync(base + NA_OFF_F, 0, NA_NODAL, s));
   CU(cudaMemsetAsync(base + NA_OFF_CNT, 0, 256, s));
+  CU(cudaMemsetAsync(base + NA_OFF_CNT + CNT_DETMIN * sizeof(unsigned long long), 0xff,
+                     sizeof(unsigned long long), s));
   const unsigned ngrid = (unsigned)ceil_div(npoin, 256);
   k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_coord, (double*)(base + NA_OFF_COORD), npoin, NA_NPAD);
   k_aos_to_soa<<<ngrid, 256, 0, s>>>(d_displ, (double*)(base + NA_OFF_U), npoin, NA_NPAD);
@@ -1795,5 +1911,117 @@ extern "C" int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int3
   if (rc) return rc;
   k_soa_to_aos<<<ngrid, 256, 0, s>>>((const double*)(base + NA_OFF_F), d_rhsid, npoin, NA_NPAD);
   CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+// The counters of the last sma_assemble_noalloc call on the current device,
+// read from the fixed array on `stream` (synchronised): return-map
+// activations and failures, both transformations active, Gauss points with
+// det F <= 0 with the smallest such det F and its element, in the numbering
+// the caller passed (the no-alloc path keeps it).
+extern "C" int32_t sma_noalloc_counters(sma_counters* out, void* stream) {
+  if (!out) return fail(SMA_ERR_ARG, "NULL argument");
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !g_noalloc_ptr[dev])
+    return fail(SMA_ERR_STATE, "no sma_assemble_noalloc call on this device yet");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned long long h[NCNT];
+  CU(cudaMemcpyAsync(h, g_noalloc_ptr[dev] + NA_OFF_CNT, sizeof h, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int k = 0; k < SMA_NCOUNTERS; ++k) out->c[k] = (k < CNT_DETMIN) ? (int64_t)h[k] : 0;
+  const unsigned long long dm = h[CNT_DETMIN];
+  if (dm == ~0ull) {
+    out->gpdet_min = 0.0;
+    out->ielem_min = -1;
+  } else {
+    const unsigned key = (unsigned)(dm >> 32);
+    const unsigned bits = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+    float det;
+    std::memcpy(&det, &bits, sizeof det);
+    out->gpdet_min = det;
+    out->ielem_min = (int64_t)(dm & 0xffffffffull);
+  }
+  return SMA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the learned surrogate in the element loop
+// ---------------------------------------------------------------------------
+extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_sur_stats* stats, double gate,
+                                     double xs_tol, int32_t enable) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  CU(cudaSetDevice(c->dev));
+  if (!enable) {
+    if (c->sur) destroy_graphs(c);
+    c->sur = false;
+    return SMA_OK;
+  }
+  if (!params || !stats) return fail(SMA_ERR_ARG, "NULL argument");
+  if (c->prec != SMA_PREC_FP32) return fail(SMA_ERR_ARG, "the surrogate runs in the FP32 precision form");
+  if (c->scatter != SMA_SCATTER_ATOMIC) return fail(SMA_ERR_ARG, "the surrogate element loop scatters by atomics");
+  if (c->damp) return fail(SMA_ERR_ARG, "the surrogate element loop has no Rayleigh damping");
+  if (c->d_lmate && !c->compact)
+    return fail(SMA_ERR_ARG, "per-element materials need compact records for the surrogate");
+  if (!(gate > 0.0) || !(xs_tol >= 0.0)) return fail(SMA_ERR_ARG, "gate > 0, xs_tol >= 0");
+  for (int k = 0; k < SMA_SUR_NPARAM; ++k)
+    if (!std::isfinite(params[k])) return fail(SMA_ERR_ARG, "non-finite surrogate parameter");
+  int32_t rc;
+  if (!c->d_sur_img) {
+    if ((rc = dalloc(&c->d_sur_img, sur::IMG_BYTES))) return rc;
+    if ((rc = dalloc(&c->d_sur_stats, sizeof(sur::SurStats)))) return rc;
+    if ((rc = dalloc(&c->d_sur_ctr, 2 * sizeof(int)))) return rc;
+    for (int b = 0; b < 2; ++b)
+      if ((rc = dalloc(&c->d_etr[b], 6 * (size_t)c->sst * sizeof(float)))) return rc;
+    CU(cudaFuncSetAttribute(sur::k_element_sur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sur::sur_elem_smem_bytes()));
+    CU(cudaFuncSetAttribute(sur::k_element_sur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sur::sur_elem_smem_bytes()));
+  }
+  // parameters through the staging buffer (>= 14,608 floats for any mesh of
+  // at least 1,218 nodes; else a temporary), packed into the weight image
+  float* d_w = nullptr;
+  const bool stage = 3 * (size_t)c->npoin * sizeof(double) >= SMA_SUR_NPARAM * sizeof(float);
+  if (stage) d_w = reinterpret_cast<float*>(c->d_stage);
+  else if ((rc = dalloc(&d_w, SMA_SUR_NPARAM * sizeof(float)))) return rc;
+  CU(cudaMemcpyAsync(d_w, params, SMA_SUR_NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaMemsetAsync(c->d_sur_img, 0, sur::IMG_BYTES, c->stream));
+  sur::k_sur_pack_image<<<(sur::HID * sur::HID + 255) / 256, 256, 0, c->stream>>>(d_w, c->d_sur_img);
+  CU(cudaMemcpyAsync(c->d_sur_stats, stats, sizeof(sur::SurStats), cudaMemcpyHostToDevice, c->stream));
+  CU(cudaMemsetAsync(c->d_sur_ctr, 0, 2 * sizeof(int), c->stream));
+  // eps_tr of the TIME_N state at the current displacement
+  {
+    ElemArgs<float> a = elem_args<float>(c, 0, c->nelem, false, false);
+    const unsigned grid = (unsigned)ceil_div(c->nelem, 16);
+    if (c->compact) sur::k_sur_etr_init<true><<<grid, 128, 0, c->stream>>>(a, c->d_etr[c->cur]);
+    else sur::k_sur_etr_init<false><<<grid, 128, 0, c->stream>>>(a, c->d_etr[c->cur]);
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(c->stream));
+  if (!stage) cudaFree(d_w);
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, c->compact ? sur::k_element_sur<true>
+                                                                       : sur::k_element_sur<false>,
+                                                   sur::SUR_BLOCK, sur::sur_elem_smem_bytes()));
+  if (per_sm < 1) return fail(SMA_ERR_ARG, "surrogate element kernel does not fit on an SM");
+  c->sur_grid = c->nsm * per_sm;
+  c->sur_gate = (float)gate;
+  c->sur_xs_tol = (float)xs_tol;
+  destroy_graphs(c);
+  c->sur = true;
+  return SMA_OK;
+}
+
+// status of the surrogate element loop since it was switched on: 1 if a wait
+// for the tensor cores ran out (the results of that launch are incomplete)
+extern "C" int32_t sma_surrogate_status(sma_ctx* c, int32_t* status) {
+  if (!c || !status) return fail(SMA_ERR_ARG, "NULL argument");
+  if (!c->d_sur_ctr) {
+    *status = 0;
+    return SMA_OK;
+  }
+  CU(cudaSetDevice(c->dev));
+  CU(cudaMemcpyAsync(status, c->d_sur_ctr + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
   return SMA_OK;
 }

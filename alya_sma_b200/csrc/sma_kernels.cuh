@@ -125,9 +125,65 @@ struct ElemArgs {
   double grav[3];              // rho-scaled body force per unit mass (elfext)
   int has_grav;
   const double* vel;           // SoA [3][npad] velocity for Rayleigh alpha, or null
-  MatC mat0;                   // the material when lmate is null (kernel-parameter space)
+  MatC mat0;                   // the material when lmate is null (kernel-parameter space);
+                               // with compact records the values every element shares
   int64_t pf_ahead;            // elements ahead whose connectivity is prefetched to L2 (0: none)
+  const T* matx;               // compact per-element records [nelem][MATX] (internal order), or null
 };
+
+// Compact per-element material record: the values a mesh whose elements
+// differ only in their moduli,
+// transformation strain and thresholds needs per element (the ensemble's and
+// the cylinder's sampled materials), and the element's temperature.  The
+// shared values (nu-derived factors, alpha, Clausius-Clapeyron slopes,
+// density, Rayleigh alpha) stay in ElemArgs::mat0.  The Young's modulus
+// enters through the Reuss rule E(xS0) = 1 / ((1 - xS0)/E_A + xS0/E_M),
+// which is E_A when E_M = E_A.  FP64 forms store the values; FP32 forms store
+// their offsets from mat0's (temperature: from mat0.T0) in FP32, 32 bytes
+// per element, whose rounding (relative 6e-8 of an offset of ~10 %) stays
+// an order below FP32 rounding of the values themselves: with the values
+// rounded to FP32 the thresholds and temperature moved the step at which
+// Gauss points start transforming, and the 2.0 M-element cylinder's 300-step
+// FP32 trajectory parted from the FP64 oracle by 2e-5 instead of 2.5e-6.
+enum MatX { MX_IEA = 0, MX_IEM, MX_EL, MX_RS_AS, MX_RF_AS, MX_RS_SA, MX_RF_SA, MX_TEMP, MATX };
+
+// the element's material from its compact record: mat0's shared values,
+// the record's own (8 lanes of an element read the same 8 words)
+template <typename T>
+__device__ __forceinline__ MatC compact_mat(const ElemArgs<T>& a, int64_t ec, double* tmp) {
+  double r[MATX];
+  const T* src = a.matx + MATX * ec;
+  MatC m = a.mat0;
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int k = 0; k < MATX; k += 2) {
+      const double2 v = __ldg(reinterpret_cast<const double2*>(src + k));
+      r[k] = v.x;
+      r[k + 1] = v.y;
+    }
+  } else {
+    const float4 v0 = __ldg(reinterpret_cast<const float4*>(src));
+    const float4 v1 = __ldg(reinterpret_cast<const float4*>(src + 4));
+    r[MX_IEA] = m.iEA + (double)v0.x;
+    r[MX_IEM] = m.iEM + (double)v0.y;
+    r[MX_EL] = m.eL + (double)v0.z;
+    r[MX_RS_AS] = m.Rs_AS + (double)v0.w;
+    r[MX_RF_AS] = m.Rf_AS + (double)v1.x;
+    r[MX_RS_SA] = m.Rs_SA + (double)v1.y;
+    r[MX_RF_SA] = m.Rf_SA + (double)v1.z;
+    r[MX_TEMP] = m.T0 + (double)v1.w;
+  }
+  m.iEA = r[MX_IEA];
+  m.iEM = r[MX_IEM];
+  m.eL = r[MX_EL];
+  m.Rs_AS = r[MX_RS_AS];
+  m.Rf_AS = r[MX_RF_AS];
+  m.Rs_SA = r[MX_RS_SA];
+  m.Rf_SA = r[MX_RF_SA];
+  m.ext_E = 1;
+  *tmp = r[MX_TEMP];
+  return m;
+}
 
 // Shared memory of one element (8 lanes): node data as structure of arrays
 // (phase 1 reads all 8 nodes of one component with 128-bit loads), and the
@@ -285,42 +341,14 @@ __device__ __forceinline__ T gp_kinematics(const T* nsm, int g, T* Ji, T* H, T* 
   return det8 * T(1.0 / 512.0);
 }
 
-// Work of one lane (element le, lane a) on one tile once its node is
-// gathered: dX, dU are node a's coordinates and displacement relative to the
-// element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
-// Gauss point a, `mat` the element's material (the kernel parameter for a
-// one-material mesh, so its constants are instruction operands; a shared-
-// memory copy otherwise), `tmp` its temperature and Vn node a's velocity
-// (read only in the DAMP instance, which adds the Rayleigh alpha force; the
-// others keep the register budget of the undamped step).  Stages the node
-// rows, then phase 1 (lane = Gauss point), the law, phase 2 (lane = node) and
-// the scatter-add.  Needs the block's reference table in `tab`.
-template <typename T, bool ATOMIC, bool DAMP = false>
-__device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab, T* nsm, T* qsm,
-                                             int lane8, bool valid, int64_t ec, int nid,
-                                             const double* dX, const double* dU,
-                                             double xS, double F_AS, double F_SA,
-                                             const MatC& mat, double tmp, const T* Vn) {
-  {
-    const T v[6] = {(T)dX[0], (T)dX[1], (T)dX[2], (T)dU[0], (T)dU[1], (T)dU[2]};
-    stage_node_rows<T>(nsm, lane8, v);
-  }
-  const int64_t gp = 8 * ec + lane8;
-  __syncwarp();                                                  // node rows of the element
-
-  // ---- phase 1, lane = Gauss point g ------------------------------------
-  T Ji[9], H[9], Jc[9];                                          // Jc = 8 F J, live across the law
-  const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H, Jc);
-
-  // ---- constitutive update ----------------------------------------------
-  T tau[6];
-  const int flag = law160_tau<T>(mat, H, tmp, xS, F_AS, F_SA, tau);
-  if (valid) {
-    a.snew[gp] = (T)xS;
-    a.snew[a.sst + gp] = (T)F_AS;
-    a.snew[2 * a.sst + gp] = (T)F_SA;
-  }
-
+// Phase 2 of a tile once the Kirchhoff stress tau of this lane's Gauss point
+// is known: the force operator Q = vol tau (F J)^-T in shared memory, then
+// lane = node a sums f_a = -sum_g Q_g dN_a(g) (+ the body force) and
+// scatters it (FP64 atomics or read-modify-write).  Jc = 8 F J.  Returns
+// det(8 F J).
+template <typename T, bool ATOMIC, bool DAMP>
+__device__ __forceinline__ T tile_forces(const ElemArgs<T>& a, const T* tab, T* qsm, int lane8, bool valid, int nid,
+                                         const T* tau, const T* Jc, T detJ, const MatC& mat, const T* Vn) {
   // ---- force operator Q = vol tau (F J)^-T, f_a = -Q dN_a ---------------
   T B[9];                                                        // B = (8 F J)^-1 = dxi/dx / 8
   const T detFJ = inv3(Jc, B);                                   // det F = det(8 F J) / (512 det J)
@@ -394,6 +422,46 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
       dst[2 * a.npad] += (double)f2;
     }
   }
+  return detFJ;
+}
+
+// Work of one lane (element le, lane a) on one tile once its node is
+// gathered: dX, dU are node a's coordinates and displacement relative to the
+// element's first node (formed in FP64), (xS, F_AS, F_SA) the TIME_N state of
+// Gauss point a, `mat` the element's material (the kernel parameter for a
+// one-material mesh, so its constants are instruction operands; a shared-
+// memory copy otherwise), `tmp` its temperature and Vn node a's velocity
+// (read only in the DAMP instance, which adds the Rayleigh alpha force; the
+// others keep the register budget of the undamped step).  Stages the node
+// rows, then phase 1 (lane = Gauss point), the law, phase 2 (lane = node) and
+// the scatter-add.  Needs the block's reference table in `tab`.
+template <typename T, bool ATOMIC, bool DAMP = false>
+__device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab, T* nsm, T* qsm,
+                                             int lane8, bool valid, int64_t ec, int nid,
+                                             const double* dX, const double* dU,
+                                             double xS, double F_AS, double F_SA,
+                                             const MatC& mat, double tmp, const T* Vn) {
+  {
+    const T v[6] = {(T)dX[0], (T)dX[1], (T)dX[2], (T)dU[0], (T)dU[1], (T)dU[2]};
+    stage_node_rows<T>(nsm, lane8, v);
+  }
+  const int64_t gp = 8 * ec + lane8;
+  __syncwarp();                                                  // node rows of the element
+
+  // ---- phase 1, lane = Gauss point g ------------------------------------
+  T Ji[9], H[9], Jc[9];                                          // Jc = 8 F J, live across the law
+  const T detJ = gp_kinematics<T>(nsm, lane8, Ji, H, Jc);
+
+  // ---- constitutive update ----------------------------------------------
+  T tau[6];
+  const int flag = law160_tau<T>(mat, H, tmp, xS, F_AS, F_SA, tau);
+  if (valid) {
+    a.snew[gp] = (T)xS;
+    a.snew[a.sst + gp] = (T)F_AS;
+    a.snew[2 * a.sst + gp] = (T)F_SA;
+  }
+
+  const T detFJ = tile_forces<T, ATOMIC, DAMP>(a, tab, qsm, lane8, valid, nid, tau, Jc, detJ, mat, Vn);
   count_warp(a.cnt, CNT_NR_ACTIVE, valid && (flag & (NR_CONVERGED | NR_FAILED)));
   // the rare events behind one vote: failed return map, both transformations,
   // det F <= 0 (det F = det(8 F J) / (512 det J))
@@ -406,6 +474,7 @@ __device__ __forceinline__ void element_tile(const ElemArgs<T>& a, const T* tab,
       atomicMin(a.cnt + CNT_DETMIN, detmin_key((float)(detFJ / (T(512) * detJ)), ec));
   }
 }
+
 
 // a material is copied as MAT_CHUNKS 16-byte chunks by the 8 lanes of its element
 constexpr int MAT_CHUNKS = (int)(sizeof(MatC) / 16);
@@ -436,11 +505,13 @@ __device__ __forceinline__ const MatC& elem_mat(const ElemArgs<T>& a, const MatC
 //     168 registers at 12 warps lost 17 % on the FP64 cantilever;
 //   256-thread blocks with per-element materials or FP64, and the pipelined
 //     kernel: 2 x 256 (128 registers).
-template <typename T, bool PIPE, bool MATS, bool NARROW = false>
+//   compact per-element records (CMP): no shared-memory material, no block
+//     barrier: the one-material caps.
+template <typename T, bool PIPE, bool MATS, bool NARROW = false, bool CMP = false>
 constexpr int elem_min_blocks() {
   if (PIPE) return 2;
-  if (NARROW) return MATS ? 5 : (sizeof(T) == 4 ? 7 : 6);
-  return (sizeof(T) == 4 && !MATS) ? 3 : 2;
+  if (NARROW) return (MATS && !CMP) ? 5 : (sizeof(T) == 4 ? 7 : 6);
+  return (sizeof(T) == 4 && (!MATS || CMP)) ? 3 : 2;
 }
 constexpr int ELEM_NARROW_BLOCK = 128;
 
@@ -457,9 +528,13 @@ constexpr int ELEM_NARROW_BLOCK = 128;
 // cantilever (4.1 % of it with the prefetch compiled in but not taken, from
 // the instruction schedule around it); with per-element materials it was
 // -1.2 % on the cylinder and +1.3 % on the 256-specimen ensemble, so off.
-template <typename T, bool ATOMIC, bool MATS, bool DAMP = false, bool NARROW = false>
+// CMP (with MATS): the element's material from its compact record in
+// registers (compact_mat), the reference table from the constant array, no
+// shared-memory material and no block barrier.
+template <typename T, bool ATOMIC, bool MATS, bool DAMP = false, bool NARROW = false, bool CMP = false>
 __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
-                                  (elem_min_blocks<T, false, MATS, NARROW>())) k_element(ElemArgs<T> a) {
+                                  (elem_min_blocks<T, false, MATS, NARROW, CMP>())) k_element(ElemArgs<T> a) {
+  constexpr bool STAGE = MATS && !CMP;                           // material and table through shared memory
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tab_sm = reinterpret_cast<T*>(smem_raw);                    // [8][8][4]
   T* elem_sm = tab_sm + 256;
@@ -474,8 +549,8 @@ __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
   MatC* msm = reinterpret_cast<MatC*>(elem_sm + epb * ElemSmem<T>::PER_ELEM) + le;
 
   if (a.ts && blockIdx.x == 0 && threadIdx.x == 0) advance_time(a.ts, a.ft);
-  if constexpr (MATS) fill_hex8_table<T>(tab_sm);
-  if constexpr (!MATS) {
+  if constexpr (STAGE) fill_hex8_table<T>(tab_sm);
+  if constexpr (!STAGE) {
     // the connectivity of the element one resident wave ahead, into L2, so
     // the block that gathers it there starts from an L2 hit
     if (a.pf_ahead) {
@@ -485,8 +560,11 @@ __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
   }
 
   const int nid = a.lnods[8 * ec + lane8];
-  const double tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
-  if constexpr (MATS) {
+  double tmp = 0.0;
+  MatC mx;
+  if constexpr (CMP) mx = compact_mat<T>(a, ec, &tmp);
+  else tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
+  if constexpr (STAGE) {
     const uint4* src = reinterpret_cast<const uint4*>(a.mats + __ldg(a.lmate + ec));
     uint4* dst = reinterpret_cast<uint4*>(msm);
     dst[lane8] = __ldg(src + lane8);
@@ -512,9 +590,13 @@ __global__ void __launch_bounds__(NARROW ? ELEM_NARROW_BLOCK : 256,
 #pragma unroll
     for (int c = 0; c < 3; ++c) Vn[c] = (T)__ldg(a.vel + c * a.npad + nid);
   }
-  if constexpr (MATS) __syncthreads();                           // reference table, materials
-  element_tile<T, ATOMIC, DAMP>(a, MATS ? tab_sm : hex8_tab<T>(), nsm, qsm, lane8, valid, ec, nid, dX, dU,
-                                xS, F_AS, F_SA, elem_mat<MATS>(a, msm), tmp, Vn);
+  if constexpr (STAGE) __syncthreads();                          // reference table, materials
+  if constexpr (CMP)
+    element_tile<T, ATOMIC, DAMP>(a, hex8_tab<T>(), nsm, qsm, lane8, valid, ec, nid, dX, dU, xS, F_AS, F_SA,
+                                  mx, tmp, Vn);
+  else
+    element_tile<T, ATOMIC, DAMP>(a, STAGE ? tab_sm : hex8_tab<T>(), nsm, qsm, lane8, valid, ec, nid, dX, dU,
+                                  xS, F_AS, F_SA, elem_mat<MATS>(a, msm), tmp, Vn);
 }
 
 // ---------------------------------------------------------------------------
@@ -1143,7 +1225,8 @@ __global__ void k_rayleigh(const int32_t* lnods, const double* coord, const doub
     for (int c = 0; c < 3; ++c) atomicAdd(fray + c * npad + nd[b], f[b][c]);
 }
 
-// state layout: reference (3, 8, 2, nelem) <-> SoA [3][sst] per slot
+// state layout: reference (3, 8, 2, nelem) <-> SoA [3][sst] per slot; a
+// null slot pointer leaves that slot alone (not read, not written)
 template <typename T>
 __global__ void k_state_in(const double* host_layout, const int32_t* perm, T* s_iterk,
                            T* s_timen, int64_t nelem, int64_t sst) {
@@ -1153,8 +1236,8 @@ __global__ void k_state_in(const double* host_layout, const int32_t* perm, T* s_
   const int64_t ue = perm ? perm[e] : e;
   const double* src = host_layout + 48 * ue;
   for (int c = 0; c < 3; ++c) {
-    s_iterk[c * sst + i] = (T)src[c + 3 * g];
-    s_timen[c * sst + i] = (T)src[24 + c + 3 * g];
+    if (s_iterk) s_iterk[c * sst + i] = (T)src[c + 3 * g];
+    if (s_timen) s_timen[c * sst + i] = (T)src[24 + c + 3 * g];
   }
 }
 template <typename T>
@@ -1166,8 +1249,8 @@ __global__ void k_state_out(double* host_layout, const int32_t* perm, const T* s
   const int64_t ue = perm ? perm[e] : e;
   double* dst = host_layout + 48 * ue;
   for (int c = 0; c < 3; ++c) {
-    dst[c + 3 * g] = (double)s_iterk[c * sst + i];
-    dst[24 + c + 3 * g] = (double)s_timen[c * sst + i];
+    if (s_iterk) dst[c + 3 * g] = (double)s_iterk[c * sst + i];
+    if (s_timen) dst[24 + c + 3 * g] = (double)s_timen[c * sst + i];
   }
 }
 

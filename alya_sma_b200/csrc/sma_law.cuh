@@ -47,7 +47,7 @@ struct MatC {
   int ext_E;                    // 1: E depends on xS0
   int pad;
   double ray_a;                 // Rayleigh alpha (mass-proportional damping), 0: none
-  double pad2;
+  double T0;                    // base temperature of compact per-element records
 };
 
 // ---------------------------------------------------------------------------
@@ -259,22 +259,20 @@ __device__ __forceinline__ RMOut return_map(const MatC& m, double K, double G, d
 }
 
 // ---------------------------------------------------------------------------
-// Kirchhoff stress of law 160 from H = F - I (row-major).  state = (xS, F_AS,
-// F_SA) of the previous step; on return the new state.  tau as
-// (xx, yy, zz, xy, yz, xz).
+// Law 160 from A = b - I (spatial frame: tau, the Kirchhoff stress) or from
+// A = C - I = 2E (material frame: the rotated-back Kirchhoff stress
+// R^T tau R, whose pull-back C^-1 (R^T tau R) is the second Piola-Kirchhoff
+// stress, since it is coaxial with C).  b and C share their eigenvalues, so
+// the return map is the same.  state = (xS, F_AS, F_SA) of the previous
+// step; on return the new state.  Tensors as (xx, yy, zz, xy, yz, xz).
+// dir, if not null, receives the unit deviatoric direction e / |e| of the
+// logarithmic strain in the same frame (zero when |e| is below FP64 epsilon).
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
-                                          double& xS, double& F_AS, double& F_SA, T* tau) {
+__device__ __forceinline__ int law160_from_A(const MatC& m, const T* A, double tmp,
+                                             double& xS, double& F_AS, double& F_SA, T* tau,
+                                             T* dir = nullptr) {
   using M = Fm<T>;
-  // A = b - I = H + H^T + H H^T, H row-major (H[3i+j] = du_i/dX_j)
-  T A[6];
-  A[0] = T(2) * H[0] + (H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
-  A[1] = T(2) * H[4] + (H[3] * H[3] + H[4] * H[4] + H[5] * H[5]);
-  A[2] = T(2) * H[8] + (H[6] * H[6] + H[7] * H[7] + H[8] * H[8]);
-  A[3] = H[1] + H[3] + (H[0] * H[3] + H[1] * H[4] + H[2] * H[5]);   // (0,1)
-  A[4] = H[5] + H[7] + (H[3] * H[6] + H[4] * H[7] + H[5] * H[8]);   // (1,2)
-  A[5] = H[2] + H[6] + (H[0] * H[6] + H[1] * H[7] + H[2] * H[8]);   // (0,2)
   T L[6], f[3];
   sym_log1p(A, L, f);
   // logarithmic strains (:313-332): ln(lambda_i) = f_i/2
@@ -307,7 +305,70 @@ __device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
   tau[3] = kh * L[3];
   tau[4] = kh * L[4];
   tau[5] = kh * L[5];
+  if (dir) {
+    // e = L/2 - theta/3 I
+    const T ie = (en_t > T(2.220446049250313e-16)) ? M::rcp(en_t) : T(0);
+    const T h = T(0.5) * ie, d0 = t3 * ie;
+    dir[0] = h * L[0] - d0;
+    dir[1] = h * L[1] - d0;
+    dir[2] = h * L[2] - d0;
+    dir[3] = h * L[3];
+    dir[4] = h * L[4];
+    dir[5] = h * L[5];
+  }
   return r.flag;
+}
+
+// Kirchhoff stress of law 160 from H = F - I (row-major, H[3i+j] =
+// du_i/dX_j): the spatial frame, A = b - I = H + H^T + H H^T
+template <typename T>
+__device__ __forceinline__ int law160_tau(const MatC& m, const T* H, double tmp,
+                                          double& xS, double& F_AS, double& F_SA, T* tau) {
+  T A[6];
+  A[0] = T(2) * H[0] + (H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
+  A[1] = T(2) * H[4] + (H[3] * H[3] + H[4] * H[4] + H[5] * H[5]);
+  A[2] = T(2) * H[8] + (H[6] * H[6] + H[7] * H[7] + H[8] * H[8]);
+  A[3] = H[1] + H[3] + (H[0] * H[3] + H[1] * H[4] + H[2] * H[5]);   // (0,1)
+  A[4] = H[5] + H[7] + (H[3] * H[6] + H[4] * H[7] + H[5] * H[8]);   // (1,2)
+  A[5] = H[2] + H[6] + (H[0] * H[6] + H[1] * H[7] + H[2] * H[8]);   // (0,2)
+  return law160_from_A<T>(m, A, tmp, xS, F_AS, F_SA, tau);
+}
+
+// A = C - I = 2E = H + H^T + H^T H (the material frame)
+template <typename T>
+__device__ __forceinline__ void green_2E(const T* H, T* A) {
+  A[0] = T(2) * H[0] + (H[0] * H[0] + H[3] * H[3] + H[6] * H[6]);
+  A[1] = T(2) * H[4] + (H[1] * H[1] + H[4] * H[4] + H[7] * H[7]);
+  A[2] = T(2) * H[8] + (H[2] * H[2] + H[5] * H[5] + H[8] * H[8]);
+  A[3] = H[1] + H[3] + (H[0] * H[1] + H[3] * H[4] + H[6] * H[7]);   // (0,1)
+  A[4] = H[5] + H[7] + (H[1] * H[2] + H[4] * H[5] + H[7] * H[8]);   // (1,2)
+  A[5] = H[2] + H[6] + (H[0] * H[2] + H[3] * H[5] + H[6] * H[8]);   // (0,2)
+}
+
+// inverse of a symmetric 3x3 (xx, yy, zz, xy, yz, xz)
+template <typename T>
+__device__ __forceinline__ void sym_inv3(const T* S, T* Si) {
+  const T c00 = S[1] * S[2] - S[4] * S[4];
+  const T c01 = S[4] * S[5] - S[3] * S[2];
+  const T c02 = S[3] * S[4] - S[1] * S[5];
+  const T id = Fm<T>::rcp(S[0] * c00 + S[3] * c01 + S[5] * c02);
+  Si[0] = c00 * id;
+  Si[1] = (S[0] * S[2] - S[5] * S[5]) * id;
+  Si[2] = (S[0] * S[1] - S[3] * S[3]) * id;
+  Si[3] = c01 * id;
+  Si[4] = (S[3] * S[5] - S[0] * S[4]) * id;
+  Si[5] = c02 * id;
+}
+
+// product of two commuting symmetric 3x3 (the result is symmetric)
+template <typename T>
+__device__ __forceinline__ void sym_mul_commuting(const T* A, const T* B, T* P) {
+  P[0] = A[0] * B[0] + A[3] * B[3] + A[5] * B[5];
+  P[1] = A[3] * B[3] + A[1] * B[1] + A[4] * B[4];
+  P[2] = A[5] * B[5] + A[4] * B[4] + A[2] * B[2];
+  P[3] = A[0] * B[3] + A[3] * B[1] + A[5] * B[4];
+  P[4] = A[3] * B[5] + A[1] * B[4] + A[4] * B[2];
+  P[5] = A[0] * B[5] + A[3] * B[4] + A[5] * B[2];
 }
 
 // inverse and determinant of a general 3x3 (row-major M[3*i+j])

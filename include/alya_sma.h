@@ -62,7 +62,8 @@ extern "C" {
 #define SMA_CNT_NR_BOTH     2   /* AS and SA active together                    */
 #define SMA_CNT_NEG_DET     3   /* Gauss points with det F <= 0                 */
 #define SMA_CNT_NONFINITE   4   /* non-finite nodal accelerations               */
-                            /* 5..7: reserved, read as 0                     */
+                            /* 5, 7: surrogate counters (sma_set_surrogate);
+                             * 6: reserved, read as 0                        */
 #define SMA_NCOUNTERS       8
 
 typedef struct sma_ctx sma_ctx;
@@ -111,7 +112,10 @@ typedef struct {
 /* element-loop kernels */
 #define SMA_VARIANT_AUTO    0   /* PLAIN in both precisions (measured on B200)                */
 #define SMA_VARIANT_PIPE    1   /* persistent blocks, next tile's gather in flight (cp.async) */
-#define SMA_VARIANT_PLAIN   2   /* one tile per block                                        */
+#define SMA_VARIANT_PLAIN   2   /* one tile per block; per-element materials that differ only */
+                                /* in E_A, E_M, eL and thresholds as compact 8-word records   */
+#define SMA_VARIANT_TABLE   3   /* one tile per block, per-element materials staged from the  */
+                                /* full material table through shared memory                  */
 
 /* explicit schemes (TIME_INTEGRATION of sld_reanut.f90:118-184) */
 #define SMA_SCHEME_CD       0   /* central difference, mod_sld_solution_methods.f90:101-223 */
@@ -198,23 +202,123 @@ int32_t sma_eval_law160_tangent(int64_t n, const double* props, double e_mart,
  * synchronise the device or exceed the caller's memory budget).  Inputs and
  * outputs are caller-owned device pointers: lnods (8,nelem) with node ids in
  * [0,npoin), coord and displ (3,npoin), sdv (3,8,2,nelem) read at slot
- * TIME_N and written at slot ITER_K, rhsid (3,npoin) = f_ext - f_int of the
- * element loop (no nodal loads); props is a host array of 18 doubles.
+ * TIME_N and written at slot ITER_K only (slot TIME_N is left bit for bit
+ * as it was), rhsid (3,npoin) = f_ext - f_int of the element loop (no nodal
+ * loads); props is a host array of 18 doubles.
  * The working set lives in one fixed device array compiled into the
  * library (about 7.5 MB, held by every GPU that loads the library until the
  * process exits), so meshes are limited to SMA_NOALLOC_MAX_ELEMS elements and
  * SMA_NOALLOC_MAX_NODES nodes; larger ones return SMA_ERR_ARG.  The first
- * call on a device looks up that array's device address (make it before any
- * stream capture on that device); every call validates lnods with one host
- * synchronisation.  All calls share the array: calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialised by the
- * caller.  Ordered on `stream` (NULL: default stream). */
+ * call on a device does the set-up: it looks up that array's device address
+ * and, since CUDA loads a library's device code on first use (lazy module
+ * loading), it may load the module, which allocates and synchronises -- make
+ * that first call during initialisation, before any stream capture on the
+ * device.  Every call then validates lnods with one host synchronisation on
+ * `stream`, so no call may be made while `stream` is being captured into a
+ * CUDA graph.  All calls share the array, which keeps the previous call's
+ * contents (the accumulators and counters are cleared by each call): calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller.  Ordered on `stream` (NULL: default stream).
+ * The return-map and det F <= 0 counters of the last call are read with
+ * sma_noalloc_counters. */
 #define SMA_NOALLOC_MAX_NODES 16384
 #define SMA_NOALLOC_MAX_ELEMS 16384
 int32_t sma_assemble_noalloc(int32_t nelem, int32_t npoin, const int32_t* d_lnods,
                              const double* d_coord, const double* d_displ,
                              const double* props, double e_mart, double* d_sdv,
                              double* d_rhsid, int32_t precision, void* stream);
+/* Counters of the last sma_assemble_noalloc call on the current device (the
+ * sld_detjac report of the reference, sld_elmpre.f90:229-238, and its
+ * return-map warnings, sld_stress_model_160.f90:377-379, 459-465), read on
+ * `stream` with one host synchronisation; ielem_min in the caller's element
+ * numbering.  SMA_ERR_STATE before the first call on the device. */
+int32_t sma_noalloc_counters(sma_counters* out, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Learned constitutive surrogate of law 160.  No counterpart in the
+ * reference (its adjacent hook is the ANN framework's libtorch forward pass,
+ * src/alya-ann/mod_ann_framework.f90:421-446, eval_r1); the law it stands in
+ * for is compute_kirchoff_stress, sld_stress_model_160.f90:212-500.
+ * Network 14 -> 64 -> 64 -> 64 -> 64 -> 13 (SiLU), BF16 weights with FP32
+ * accumulation on the tensor cores, per Gauss point in the material frame
+ * (tensors xx, yy, zz, xy, yz, xz):
+ *   x: Green-Lagrange strain E (6), previous transformation strain
+ *      eps_tr0 = eL xS0 D0 (6, D0 the unit deviatoric direction of ln U),
+ *      temperature, previous martensite fraction xS0
+ *   y: S / E(xS0) - l(E - eps_tr0) (6), xS - xS0, eps_tr - eps_tr0 (6), where
+ *      S is the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus and
+ *      l(e) = (lambda tr(e) I + 2 mu e) / E the linear-elastic stress over E.
+ * Parameters: SMA_SUR_NPARAM FP32 values, padded flat layout W1 [64][16],
+ * b1 [64], W2, W3, W4 [64][64], b2, b3, b4 [64], W5 [16][64], b5 [16]
+ * (W[o][i]: input i to output o; padding zero).  All pointers d_* are
+ * device pointers the caller owns; calls are ordered on `stream`. */
+#define SMA_SUR_NIN          14
+#define SMA_SUR_NOUT         13
+#define SMA_SUR_NPARAM       14608
+#define SMA_SUR_IMAGE_BYTES  35904   /* tcgen05 weight image (swizzled BF16 + FP32 biases) */
+typedef struct {
+  float mu_x[SMA_SUR_NIN], sd_x[SMA_SUR_NIN];    /* input normalisation            */
+  float mu_y[SMA_SUR_NOUT], sd_y[SMA_SUR_NOUT];  /* output normalisation           */
+  float linv[SMA_SUR_NIN * SMA_SUR_NIN];         /* inverse Cholesky factor of the  *
+                                                  * normalised inputs' covariance   *
+                                                  * (lower, row-major): the         *
+                                                  * out-of-envelope score is        *
+                                                  * |linv xh| / sqrt(14)            */
+} sma_sur_stats;
+
+/* Training data: npath randomised load paths of the plain law (FP64,
+ * material frame), nstep samples each, into d_x (npath*nstep, 14) and d_y
+ * (npath*nstep, 13).  Per path: the material props (18) with e_mart, its
+ * E_A, E_M, eL and four transformation stresses scaled by U(1-spread,
+ * 1+spread); a temperature U(t_lo, t_hi); a random frame; nseg linear
+ * segments between strain states with axial strain U(e_lo, e_hi), lateral
+ * contraction U(0.3, 0.5) and shear N(0, shear). */
+int32_t sma_sur_generate(int64_t npath, int32_t nstep, uint64_t seed, const double* props, double e_mart,
+                         double spread, double t_lo, double t_hi, double e_lo, double e_hi, double shear,
+                         int32_t nseg, float* d_x, float* d_y, void* stream);
+/* One training pass over a batch of n samples on the tensor cores (BF16
+ * mma.sync, FP32 accumulation): forward, backward and weight gradients of
+ * the loss mean((yh_pred - yh)^2) over samples and outputs (normalised
+ * outputs).  d_wb: BF16 weights (SMA_SUR_NPARAM, uint16 storage), d_w the
+ * FP32 master (biases are read from it); d_grad (SMA_SUR_NPARAM) and
+ * d_loss (1) are ADDED to (clear them first). */
+int32_t sma_sur_train_step(const uint16_t* d_wb, const float* d_w, const sma_sur_stats* d_stats, int64_t n,
+                           const float* d_x, const float* d_y, float* d_grad, float* d_loss, void* stream);
+/* Adam (step t >= 1) on the FP32 master weights d_w with moments d_m, d_v;
+ * writes the BF16 copy d_wb. */
+int32_t sma_sur_adam(float* d_w, float* d_m, float* d_v, const float* d_grad, uint16_t* d_wb, float lr,
+                     float b1, float b2, float eps, int32_t t, void* stream);
+/* From the FP32 master: the BF16 copy (d_wb, or NULL) and the tcgen05
+ * weight image (d_img, SMA_SUR_IMAGE_BYTES, 16-byte aligned, or NULL). */
+int32_t sma_sur_pack(const float* d_w, uint16_t* d_wb, unsigned char* d_img, void* stream);
+/* The network alone on the 5th-generation tensor cores (tcgen05.mma into
+ * tensor memory, 128 points per tile): raw d_x (n, 14) -> raw d_y (n, 13)
+ * and, if d_score is not NULL, the out-of-envelope score per point.
+ * *d_status is set to 1 if a wait for the tensor cores ran out (never
+ * expected; the results are then incomplete). */
+int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats, int64_t n, const float* d_x,
+                        float* d_y, float* d_score, int32_t* d_status, void* stream);
+/* The surrogate in a context's element loop (FP32 precision form, atomic
+ * scatter, undamped; per-element materials as compact records), in place
+ * of law 160's evaluation in sld_builtin_materials.f90:316-336: the network
+ * on the tcgen05 tensor cores for every Gauss point, then the plain law for
+ * the points the gates send back -- an out-of-envelope score above `gate`,
+ * the law's activation test (sld_stress_model_160.f90:351-374) on the
+ * loading functions of the predicted stress (a point about to transform
+ * needs the return map), or a predicted martensite increment above
+ * `xs_tol` on a point the law leaves inactive (its return-map residual is
+ * then not zero).  params: SMA_SUR_NPARAM host FP32 values, stats: host.
+ * Switching on derives eps_tr from the TIME_N state at the current
+ * displacement; enable = 0 returns to the plain law.  Counters: slot 5
+ * (SMA_CNT_SUR_FALLBACK) Gauss points sent to the plain law, slot 7
+ * (SMA_CNT_SUR_OOD) of those, out of the envelope. */
+#define SMA_CNT_SUR_FALLBACK 5
+#define SMA_CNT_SUR_OOD      7
+int32_t sma_set_surrogate(sma_ctx* ctx, const float* params, const sma_sur_stats* stats, double gate,
+                          double xs_tol, int32_t enable);
+/* 1 in *status if a wait of the surrogate element loop for the tensor cores
+ * ran out since it was switched on (never expected), else 0. */
+int32_t sma_surrogate_status(sma_ctx* ctx, int32_t* status);
 
 /* host <-> context data */
 int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);

@@ -216,6 +216,47 @@ def test_element_loop_matches_oracle(oracle, bar, precision, scatter, tol):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_compact_records_equal_the_material_table(oracle, precision):
+    """Per-element materials that differ only in E_A, E_M, eL and the
+    transformation stresses (the cylinder's sampling) run from compact 8-word
+    records in registers; SMA_VARIANT_TABLE stages each element's full
+    material through shared memory.  Both give the oracle's residual and
+    state, and each other's to round-off of the record's precision.  A mesh
+    whose materials also differ in nu cannot use the records and runs from
+    the table."""
+    import dataclasses
+    p = P.cylinder_2m(nsteps=600, div=8)
+    u = P.prestrain(p, 0.03) + np.random.default_rng(5).normal(size=p.coord.shape) * 1e-4
+    u[p.fixno == 1] = 0.0
+    o = oracle.Problem(p)
+    ro = o.assemble(u)
+    o.end_step()
+    scale = np.abs(ro["finte"]).max()
+    out = {}
+    for variant in ("plain", "table"):
+        g = sma.ExplicitSolid(p, precision=precision, scatter="color", variant=variant)
+        out[variant] = g.assemble(u)["rhsid"]
+        g.end_step()
+        out[variant + "_xs"] = g.state[:, 1, :, 0]
+        g.close()
+        tol = 1e-8 if precision == "fp64" else 1e-3
+        assert np.abs(out[variant] - ro["rhsid"]).max() / scale < tol, variant
+    d = np.abs(out["plain"] - out["table"]).max() / scale
+    assert d < (1e-12 if precision == "fp64" else 1e-5), d
+    assert np.abs(out["plain_xs"] - out["table_xs"]).max() < (1e-12 if precision == "fp64" else 1e-4)
+    # materials that also differ in Poisson's ratio: the table path
+    props = p.props.copy()
+    props[:, 1] *= np.random.default_rng(6).uniform(0.97, 1.03, size=len(props))
+    q = dataclasses.replace(p, props=props)
+    oq = oracle.Problem(q)
+    rq = oq.assemble(u)
+    g = sma.ExplicitSolid(q, precision=precision, scatter="color")
+    rg = g.assemble(u)["rhsid"]
+    assert np.abs(rg - rq["rhsid"]).max() / np.abs(rq["finte"]).max() < (1e-8 if precision == "fp64" else 1e-3)
+    g.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("mesh", ["bar", "cylinder"])
 def test_every_block_width_matches_oracle(oracle, bar, mesh, precision):
     """The element kernel is compiled twice: for blocks of at most 128 threads
@@ -364,13 +405,21 @@ def test_precision_form_cantilever(oracle):
     # peak tip displacement: the precision target 1e-4
     ipk = int(np.argmax(np.abs(h_ref)))
     rel_peak = abs(h[ipk] - h_ref[ipk]) / abs(h_ref[ipk])
-    assert rel_peak < 1e-4, rel_peak
-    # whole history: the activation test of the law (F > F0 and F > Rs) is
-    # discontinuous, so rounding-level differences shift when a Gauss point
-    # starts transforming; on this mesh two FP64 evaluations (GPU and oracle)
-    # already differ by up to 2.5e-5 over the history (1/5 resolution).
+    assert rel_peak < 1e-4, rel_peak                         # measured 1.5e-8
+    # whole history: the activation test of the law (F > F0 and F > Rs,
+    # sld_stress_model_160.f90:351,368) is discontinuous, so a rounding-level
+    # difference shifts the step at which a Gauss point starts transforming
+    # and the tip history parts by more than the rounding.  The FP64 oracle
+    # moved by one FP32 ulp of its coordinates parts from itself by
+    # 2.3e-4 over this history; the FP32 form (1.8e-4 measured) is held to
+    # the 1e-4 target or, where the law's own spread exceeds it, to twice
+    # that spread.
+    import dataclasses
+    pert = dataclasses.replace(p, coord=p.coord * (1 + 2.0 ** -24))
+    h_self = oracle.Problem(pert).run(p.dtime, 1500, wit_dof=wit)[:, 0]
+    spread = np.abs(h_self - h_ref).max() / np.abs(h_ref).max()
     rel_hist = np.abs(h - h_ref).max() / np.abs(h_ref).max()
-    assert rel_hist < 5e-4, rel_hist
+    assert rel_hist <= max(1e-4, 2.0 * spread), (rel_hist, spread)
     # stresses at the final displacement: FP32 element loop vs FP64 oracle
     u = o.displ.copy()
     g2 = sma.ExplicitSolid(p, precision="fp32")
@@ -422,6 +471,10 @@ def test_full_load_cycle_within_the_laws_own_sensitivity(oracle):
     h_self = oracle.Problem(pert).run(p.dtime, 4000, wit_dof=wit)
     scale = np.abs(h_ref).max()
     e_self = np.abs(h_self - h_ref).max(axis=1) / scale
+    # the same for a perturbation of one FP32 ulp, the precision form's scale
+    pert32 = dataclasses.replace(p, coord=p.coord * (1 + 2.0 ** -24))
+    h_self32 = oracle.Problem(pert32).run(p.dtime, 4000, wit_dof=wit)
+    e_self32 = np.abs(h_self32 - h_ref).max(axis=1) / scale
     out = {}
     for prec in ("fp64", "fp32"):
         g = sma.ExplicitSolid(p, precision=prec, scatter="color")
@@ -431,3 +484,11 @@ def test_full_load_cycle_within_the_laws_own_sensitivity(oracle):
     assert out["fp64"][:3000].max() < 1e-9                        # loading and plateau: round-off
     assert out["fp64"].max() <= 10 * e_self.max() + 1e-9           # whole cycle: the law's own spread
     assert out["fp32"][:2000].max() < 1e-4                         # precision form, loading half
+    # precision form over the whole cycle, reverse transformation included:
+    # up to every 500th step within 5x the spread of the oracle moved by one
+    # FP32 ulp, and within 2e-5 while that spread is smaller (measured on
+    # B200: 7.0e-6 / 1.0e-4 / 1.3e-3 at steps 2,000 / 3,000 / 4,000 against a
+    # spread of 5.1e-8 / 4.2e-5 / 1.4e-3)
+    for k in range(500, 4001, 500):
+        got, lim = out["fp32"][:k].max(), max(2e-5, 5.0 * e_self32[:k].max())
+        assert got <= lim, (k, got, e_self32[:k].max())

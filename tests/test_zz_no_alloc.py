@@ -2,7 +2,9 @@
 device memory (their device arrays belong to an OpenACC region or a pool of
 their own, or a cudaMalloc would synchronise the device).  Checked through
 the C ABI against the context entry point sma_assemble on two calls in a
-row, with the FP64 tolerance of the other element-loop tests.
+row, with the FP64 tolerance of the other element-loop tests; a call after
+the first allocates no device memory, leaves the caller's TIME_N state slot
+untouched, and reports its return-map and det F <= 0 counters.
 
 The file sorts last so that a run stopping at the first failure has already
 run every other test."""
@@ -30,6 +32,19 @@ def _noalloc(L):
     fn.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                    C.c_double, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
     return fn
+
+
+class _Counters(C.Structure):
+    _fields_ = [("c", C.c_int64 * 8), ("gpdet_min", C.c_double), ("ielem_min", C.c_int64)]
+
+
+def _counters(L, stream):
+    fn = L.sma_noalloc_counters
+    fn.restype = C.c_int32
+    fn.argtypes = [C.POINTER(_Counters), C.c_void_p]
+    c = _Counters()
+    assert fn(C.byref(c), stream) == 0, L.sma_last_error().decode()
+    return c
 
 
 def _field(p, strain, seed):
@@ -60,11 +75,20 @@ def test_noalloc_matches_context_entry_point(precision):
         r = ref.assemble(u)
         ref.end_step()
         displ = torch.as_tensor(u, dtype=torch.float64, device=dev).contiguous()
+        timen = sdv[:, 1].clone()
+        stream.synchronize()
+        held, free0 = torch.cuda.memory_allocated(), torch.cuda.mem_get_info()[0]
         rc = fn(p.nelem, p.npoin, lnods.data_ptr(), coord.data_ptr(), displ.data_ptr(),
                 props.ctypes.data, 0.0, sdv.data_ptr(), rhs.data_ptr(),
                 sma.PREC[precision], stream.cuda_stream)
         assert rc == 0, L.sma_last_error().decode()
         stream.synchronize()
+        if call > 0:                                        # the first call may load the module
+            assert torch.cuda.memory_allocated() == held
+            assert torch.cuda.mem_get_info()[0] == free0, "a call allocated device memory"
+        assert torch.equal(sdv[:, 1], timen), "slot TIME_N changed"
+        cnt = _counters(L, stream.cuda_stream)
+        assert cnt.c[0] > 0 and cnt.c[1] == 0 and cnt.c[3] == 0 and cnt.ielem_min == -1
         got = rhs.cpu().numpy()
         err = np.abs(got - r["rhsid"]).max() / np.abs(r["finte"]).max()
         assert err < tol, (call, err)
@@ -96,3 +120,34 @@ def test_noalloc_rejects_oversized_mesh_and_bad_ids():
     rc = fn(p.nelem, p.npoin, lnods.data_ptr(), coord.data_ptr(), coord.data_ptr(),
             props.ctypes.data, 0.0, sdv.data_ptr(), rhs.data_ptr(), 0, None)
     assert rc == -1 and b"lnods" in L.sma_last_error()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_noalloc_reports_inverted_gauss_points(precision):
+    """A node pushed through the opposite corner of its elements inverts
+    Gauss points; the counters of the call report them, with the smallest
+    det F and an element around that node, as the context path does."""
+    import torch
+    p = P.bar_40x4x4(nsteps=10, ref_equivalent=True)
+    L = sma.lib()
+    fn = _noalloc(L)
+    dev = torch.device("cuda")
+    X = p.coord
+    node = int(np.argmin(np.linalg.norm(X - np.array([20.0, 2.0, 2.0]), axis=1)))   # interior
+    u = np.zeros_like(X)
+    u[node] = (-1.6, -1.6, -1.6)
+    lnods = torch.as_tensor(p.lnods, dtype=torch.int32, device=dev).contiguous()
+    coord = torch.as_tensor(X, dtype=torch.float64, device=dev).contiguous()
+    displ = torch.as_tensor(u, dtype=torch.float64, device=dev).contiguous()
+    sdv = torch.zeros((p.nelem, 2, 8, 3), dtype=torch.float64, device=dev)
+    rhs = torch.empty((p.npoin, 3), dtype=torch.float64, device=dev)
+    props = np.ascontiguousarray(p.props[0], dtype=np.float64)
+    stream = torch.cuda.current_stream()
+    rc = fn(p.nelem, p.npoin, lnods.data_ptr(), coord.data_ptr(), displ.data_ptr(), props.ctypes.data,
+            0.0, sdv.data_ptr(), rhs.data_ptr(), sma.PREC[precision], stream.cuda_stream)
+    assert rc == 0, L.sma_last_error().decode()
+    cnt = _counters(L, stream.cuda_stream)
+    around = set(np.nonzero((p.lnods == node).any(axis=1))[0].tolist())
+    assert cnt.c[3] > 0, "no det F <= 0 reported"
+    assert cnt.gpdet_min <= 0.0
+    assert cnt.ielem_min in around
