@@ -108,6 +108,7 @@ def lib():
         L.sma_set_nodal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.sma_step_prologue.argtypes = [C.c_void_p]
         L.sma_step_elements.argtypes = [C.c_void_p]
+        L.sma_step_elements_range.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         L.sma_step_nodes.argtypes = [C.c_void_p, C.c_int32]
         L.sma_gather_residual.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.sma_scatter_residual.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]

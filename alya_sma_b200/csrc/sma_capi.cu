@@ -1157,6 +1157,50 @@ int32_t sma_step_elements(sma_ctx* c) {
   return SMA_OK;
 }
 
+// the element loop of a step in ranges, so a partitioned caller can send
+// the interface rows while the interior elements compute: first = 1 on the
+// step's first range (advances the time), last = 1 on its last (the state
+// of this step becomes TIME_N of the next)
+int32_t sma_step_elements_range(sma_ctx* c, int32_t beg, int32_t end, int32_t first, int32_t last) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (c->scatter == SMA_SCATTER_COLOR) return fail(SMA_ERR_ARG, "element ranges need the atomic scatter");
+  if (beg < 0 || end > c->nelem || beg > end) return fail(SMA_ERR_ARG, "element range outside [0, nelem)");
+  CU(cudaSetDevice(c->dev));
+  int32_t rc = SMA_OK;
+  if (first) c->last_in = c->cur;
+  if (end > beg) {
+    if (c->prec == SMA_PREC_FP32 && c->sur) {
+      rc = launch_sur_range(c, beg, end, first != 0, true);
+    } else {
+      const int epb = c->block / 8;
+      const int64_t ntiles = ceil_div(end - beg, epb);
+      const unsigned grid = c->variant == SMA_VARIANT_PIPE
+                                ? (unsigned)std::min<int64_t>(ntiles, (int64_t)c->nsm * c->resident)
+                                : (unsigned)ntiles;
+      if (c->prec == SMA_PREC_FP32) {
+        ElemArgs<float> a = elem_args<float>(c, beg, end, first != 0, true);
+        elem_kernel<float>(c)<<<grid, c->block, elem_smem<float>(c), c->stream>>>(a);
+      } else {
+        ElemArgs<double> a = elem_args<double>(c, beg, end, first != 0, true);
+        elem_kernel<double>(c)<<<grid, c->block, elem_smem<double>(c), c->stream>>>(a);
+      }
+      c->launches++;
+      CU(cudaGetLastError());
+    }
+  } else if (first) {
+    k_advance_time<<<1, 1, 0, c->stream>>>(c->d_ts, c->d_ft);
+    c->launches++;
+    CU(cudaGetLastError());
+  }
+  if (rc) return rc;
+  if (last) {
+    c->cur ^= 1;
+    if ((rc = launch_witness(c))) return rc;
+    if (c->damp && c->energy && (rc = launch_rayleigh(c, damp_velocity(c, true)))) return rc;
+  }
+  return SMA_OK;
+}
+
 int32_t sma_step_nodes(sma_ctx* c, int32_t last) {
   if (!c) return fail(SMA_ERR_ARG, "NULL context");
   CU(cudaSetDevice(c->dev));

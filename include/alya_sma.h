@@ -245,9 +245,11 @@ int32_t sma_noalloc_counters(sma_counters* out, void* stream);
  *   x: Green-Lagrange strain E (6), previous transformation strain
  *      eps_tr0 = eL xS0 D0 (6, D0 the unit deviatoric direction of ln U),
  *      temperature, previous martensite fraction xS0
- *   y: S / E(xS0) - l(E - eps_tr0) (6), xS - xS0, eps_tr - eps_tr0 (6), where
- *      S is the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus and
- *      l(e) = (lambda tr(e) I + 2 mu e) / E the linear-elastic stress over E.
+ *   y: (S - S_p) / E(xS0) (6), xS - xS0, eps_tr - eps_tr0 (6), where S is
+ *      the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus and S_p
+ *      the law's elastic response on a second-order logarithmic strain
+ *      ln U ~ E - E^2: T_p = K (tr h - 3 alpha |eps_tr0|) I + 2G (dev h -
+ *      eps_tr0), S_p = sym(C^-1 T_p).
  * Parameters: SMA_SUR_NPARAM FP32 values, padded flat layout W1 [64][16],
  * b1 [64], W2, W3, W4 [64][64], b2, b3, b4 [64], W5 [16][64], b5 [16]
  * (W[o][i]: input i to output o; padding zero).  All pointers d_* are
@@ -335,6 +337,12 @@ int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);
  * 0-based) to/from a device buffer (3, n) on the context stream. */
 int32_t sma_step_prologue(sma_ctx* ctx);
 int32_t sma_step_elements(sma_ctx* ctx);
+/* sma_step_elements in element ranges [beg, end) (atomic scatter only):
+ * first = 1 on a step's first range, last = 1 on its last, so the
+ * interface elements can run first and their shared rows cross to the
+ * neighbouring sub-meshes while the interior elements compute (the
+ * reference sums the interface after the whole loop, pararr.f90:75-162). */
+int32_t sma_step_elements_range(sma_ctx* ctx, int32_t beg, int32_t end, int32_t first, int32_t last);
 int32_t sma_step_nodes(sma_ctx* ctx, int32_t last);
 int32_t sma_gather_residual(sma_ctx* ctx, int32_t n, const int32_t* d_nodes, double* d_rows);
 int32_t sma_scatter_residual(sma_ctx* ctx, int32_t n, const int32_t* d_nodes, const double* d_rows);

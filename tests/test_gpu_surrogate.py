@@ -1,0 +1,241 @@
+"""The learned constitutive surrogate's kernels against the oracle:
+
+* the plain-law data generator (FP64, material frame) against the oracle's
+  law 160 along the same load paths;
+* the BF16 tensor-core training pass (forward, backward, weight gradients)
+  against the oracle's FP64 backpropagation on the same BF16-rounded
+  weights;
+* the tcgen05 inference against the oracle's forward pass, and its
+  out-of-envelope score against the Mahalanobis distance computed here;
+* training on generated data lowers the loss, and the trained network
+  predicts held-out plain-law stresses."""
+import numpy as np
+import pytest
+
+from alya_sma_b200 import problem as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+
+
+def _props():
+    p = P.nitinol_props(**P.NITI, C_AS=6.5 * P.SQRT_2_3, C_SA=6.5 * P.SQRT_2_3, T_ref=300.0)
+    return p, P.NITI_E_MART
+
+
+def _sym(v):
+    """(xx, yy, zz, xy, yz, xz) -> 3x3"""
+    return np.array([[v[0], v[3], v[5]], [v[3], v[1], v[4]], [v[5], v[4], v[2]]])
+
+
+def _predictor(E, etr, nu, alpha=0.0):
+    """The network's analytic stress part over E(xS0) (restated here): the
+    law's elastic response on ln U ~ E - E^2, pulled back with C^-1."""
+    kK, kG = 1 / (3 - 6 * nu), 1 / (2 + 2 * nu)
+    h = E - E @ E
+    tr = np.trace(h)
+    Tp = kK * (tr - 3 * alpha * np.linalg.norm(etr)) * np.eye(3) + 2 * kG * (h - tr / 3 * np.eye(3) - etr)
+    P = np.linalg.inv(np.eye(3) + 2 * E) @ Tp
+    return 0.5 * (P + P.T)
+
+
+def test_generator_follows_the_plain_law(oracle):
+    """Base material (no spread), one temperature.  Every sample is the
+    law's answer to a small strain increment from its path's state.  Where
+    the law's return map stayed inactive (xS unchanged) the sample depends
+    only on (E, xS0) and the current direction of ln U: replayed through the
+    oracle's law 160 at U = sqrt(I + 2E) (with F = U the spatial and material
+    frames coincide) with both activation tests forced off, S and
+    eps_tr = eL xS0 D match.  The first sample of each path starts from the
+    virgin state and is replayed with the full law."""
+    from alya_sma_b200 import surrogate as S
+    props, em = _props()
+    npath, nstep = 16, 128
+    x, y = S.generate(props, em, npath, nstep=nstep, seed=3, spread=0.0, t_range=(310.0, 310.0))
+    x, y = x.cpu().numpy().astype(np.float64), y.cpu().numpy().astype(np.float64)
+    nu = props[1]
+    worst = dict(S=0.0, xs=0.0, etr=0.0)
+    checked = transformed = 0
+    for k in range(npath * nstep):
+        first = k % nstep == 0
+        inactive = y[k, 6] == 0.0
+        if not (first or inactive):
+            continue
+        E = _sym(x[k, :6])
+        w, V = np.linalg.eigh(np.eye(3) + 2 * E)
+        U = (V * np.sqrt(w)) @ V.T
+        xs0 = x[k, 13]
+        sdv = np.zeros(3) if first else np.array([xs0, 1e30, -1e30])
+        Ex = 1.0 / ((1 - xs0) / props[0] + xs0 / em)
+        tau, sdv_new, flag = oracle.law160_kirchhoff(props, U.T.ravel(), sdv, tmp=310.0, e_mart=em)
+        tau = np.asarray(tau).reshape(3, 3).T
+        Ui = np.linalg.inv(U)
+        Sm = Ui @ tau @ Ui.T
+        S_gpu = (_sym(y[k, :6]) + _predictor(E, _sym(x[k, 6:12]), nu)) * Ex
+        worst["S"] = max(worst["S"], np.abs(S_gpu - Sm).max() / max(np.abs(Sm).max(), 1.0))
+        worst["xs"] = max(worst["xs"], abs(xs0 + y[k, 6] - sdv_new[0]))
+        lnU = (V * (0.5 * np.log(w))) @ V.T
+        dev = lnU - np.trace(lnU) / 3 * np.eye(3)
+        nrm = np.linalg.norm(dev)
+        etr = props[2] * sdv_new[0] * dev / nrm if nrm > 0 else 0 * dev
+        worst["etr"] = max(worst["etr"], np.abs(_sym(x[k, 6:12] + y[k, 7:13]) - etr).max())
+        checked += 1
+        transformed += int(xs0 > 0.05)
+    assert checked > npath * nstep // 4 and transformed > 20, (checked, transformed)
+    assert worst["S"] < 2e-4 and worst["xs"] < 1e-6 and worst["etr"] < 1e-5, worst
+    assert (y[:, 6] != 0).sum() > 0                               # some samples transform
+
+
+def _random_net(seed):
+    from alya_sma_b200 import surrogate as S
+    rng = np.random.default_rng(seed)
+    w = S.init_params(seed)
+    w[S.OFF["b1"]:S.OFF["b1"] + 64] = rng.normal(size=64) * 0.1
+    w[S.OFF["b5"]:S.OFF["b5"] + 13] = rng.normal(size=13) * 0.1
+    return w
+
+
+def _net_on_gpu(w, x, y):
+    import torch
+    from alya_sma_b200 import surrogate as S
+    net = S.Surrogate()
+    net.w.copy_(torch.from_numpy(w.astype(np.float32)))
+    net.pack()
+    net.fit_stats(x, y)
+    return net
+
+
+def test_training_gradient_matches_oracle(oracle):
+    """One training pass of the tensor-core kernel against the oracle's FP64
+    backpropagation on the same BF16-rounded weights and batch: the loss to
+    1e-2, each layer's gradient to 3e-2 in relative L2 norm."""
+    import torch
+    from alya_sma_b200 import surrogate as S
+    props, em = _props()
+    x, y = S.generate(props, em, 64, nstep=64, seed=5)
+    net = _net_on_gpu(_random_net(7), x, y)
+    n = 1000                                                  # not a multiple of the 128-sample tile
+    xb, yb = x[:n].contiguous(), y[:n].contiguous()
+    loss, g = net.gradient(xb, yb)
+    wq = net.params_bf16()
+    lo, go = oracle.mlp_loss_grad(wq, net.stats_array(), xb.cpu().numpy(), yb.cpu().numpy())
+    assert abs(loss - lo) <= 1e-2 * lo, (loss, lo)
+    keys = list(S.OFF)
+    for a, b, name in zip([S.OFF[k] for k in keys], [S.OFF[k] for k in keys[1:]] + [S.NPARAM], keys):
+        ref, got = go[a:b], g[a:b]
+        err = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
+        assert err < 3e-2, (name, err)
+
+
+def test_tcgen05_forward_matches_oracle(oracle):
+    """The tcgen05 inference (128-row tiles, TMEM accumulators) against the
+    oracle's forward pass on the same BF16-rounded weights, and its
+    out-of-envelope score against the Mahalanobis distance per dimension."""
+    import torch
+    from alya_sma_b200 import surrogate as S
+    props, em = _props()
+    x, y = S.generate(props, em, 32, nstep=64, seed=9)
+    net = _net_on_gpu(_random_net(8), x, y)
+    n = 1000
+    xb = x[:n].contiguous()
+    yg, sc = net.forward(xb)
+    yo = oracle.mlp_forward(net.params_bf16(), net.stats_array(), xb.cpu().numpy())
+    st = net.stats_array()
+    sd_y = st[28 + 13:]
+    err = np.abs(yg.cpu().numpy() - yo) / sd_y                 # in normalised output units
+    assert err.max() < 3e-2, err.max()
+    xh = (xb.cpu().numpy() - st[:14]) / st[14:28]
+    d = np.sqrt(np.sum((xh @ net.linv().T) ** 2, axis=1) / 14)
+    assert np.abs(sc.cpu().numpy() - d).max() < 1e-3 * max(1.0, d.max())
+
+
+def _trained(npath=4096, epochs=4, seed=1):
+    from alya_sma_b200 import surrogate as S
+    props, em = _props()
+    x, y = S.generate(props, em, npath, nstep=256, seed=seed, inactive_only=True)
+    net = S.Surrogate(seed=2)
+    net.fit_stats(x, y)
+    losses = net.train(x, y, epochs=epochs, batch=8192, lr=3e-3)
+    return net, losses
+
+
+def test_training_reduces_loss_and_predicts_held_out_paths(oracle):
+    """A short training run on generated plain-law paths (the points where
+    the law's return map is inactive, the ones the network stands in for):
+    the loss falls by two orders of magnitude, and on held-out paths the
+    predicted stress matches the law to 1e-3 of the stress scale (the
+    stress output is S / E(xS0) less the linear-elastic part, so its error
+    over the largest strain is the relative stress error)."""
+    from alya_sma_b200 import surrogate as S
+    net, losses = _trained()
+    assert losses[-1] < 1e-2 * losses[0], losses
+    props, em = _props()
+    xt, yt = S.generate(props, em, 256, nstep=256, seed=77, inactive_only=True)
+    yp, sc = net.forward(xt)
+    yt, yp = yt.cpu().numpy(), yp.cpu().numpy()
+    scale = np.abs(xt.cpu().numpy()[:, :6]).max()
+    err = np.abs(yp[:, :6] - yt[:, :6]).max(axis=1) / scale
+    assert np.quantile(err, 0.99) < 1e-3 and err.max() < 5e-3, (np.quantile(err, 0.99), err.max())
+    assert np.median(sc.cpu().numpy()) < 1.5
+
+
+def test_surrogate_element_loop_judged_by_the_plain_law(oracle):
+    """The surrogate in the FP32 element loop of the per-element-material
+    cylinder (div 8) with its temperature field.  The state is the plain
+    FP64 law's after 60 steps from a 1 % prestrain; at that state and
+    displacement the FP64 element loop judges the surrogate's: element
+    forces within 1e-3 of their scale (the FP32 plain loop is at ~3e-7),
+    with most Gauss points handled by the network and the transforming ones
+    sent back to the plain law.  Then 200 steps with the surrogate from
+    there stay within 1e-3 of the FP64 run's displacement."""
+    import alya_sma_b200 as sma
+    net, _ = _trained()
+    p = P.cylinder_2m(nsteps=600, div=8)
+    g64 = sma.ExplicitSolid(p, precision="fp64")
+    g64.set("displ", P.prestrain(p, 0.01))
+    g64.step(60)
+    u, state = g64.get("displ"), g64.state
+    res, cnt = {}, None
+    for k in ("fp64", "fp32", "sur"):
+        g = sma.ExplicitSolid(p, precision=("fp64" if k == "fp64" else "fp32"))
+        g.state = state
+        g.set("displ", u)
+        if k == "sur":
+            g.set_surrogate(net, gate=3.0, xs_tol=1e-3)
+        res[k] = g.assemble(u)["finte"]
+        if k == "sur":
+            cnt = g.counters()
+        g.close()
+    scale = np.abs(res["fp64"]).max()
+    e32 = np.abs(res["fp32"] - res["fp64"]).max() / scale
+    esur = np.abs(res["sur"] - res["fp64"]).max() / scale
+    ngp = 8 * p.nelem
+    assert esur < 1e-3, (esur, e32)
+    assert cnt["sur_fallback"] < 0.5 * ngp and cnt["sur_fallback"] >= cnt["nr_active"], cnt
+    # trajectories: FP64 plain and FP32 with the surrogate, both from the same state
+    gs = sma.ExplicitSolid(p, precision="fp32")
+    gs.state = state
+    gs.set("displ", u)
+    gs.set("veloc", 0 * u)
+    g64b = sma.ExplicitSolid(p, precision="fp64")
+    g64b.state = state
+    g64b.set("displ", u)
+    g64b.set("veloc", 0 * u)
+    gs.time = g64b.time = 60 * p.dtime
+    gs.set_surrogate(net)
+    gs.step(200)
+    g64b.step(200)
+    d_ref = g64b.get("displ")
+    du = np.abs(gs.get("displ") - d_ref).max() / np.abs(d_ref).max()
+    assert gs.surrogate_status() == 0
+    cs = gs.counters()
+    assert du < 1e-3, (du, cs)
+    assert cs["sur_fallback"] < 0.5 * 200 * ngp, cs
+    for g in (g64, gs, g64b):
+        g.close()
