@@ -6,9 +6,15 @@ their lumped mass summed once at set-up.
 
 The parts run in this process (``PartitionedSolid(prob, nparts)``: every
 part on ``device``, or one device each) or one per rank under
-torch.distributed (``PartitionedSolid(prob, group=...)``: NCCL all-reduce of
-the shared rows, ordered on the part's stream).  Steps use the context's
-sma_step_prologue / sma_step_elements / sma_step_nodes, the same kernels as
+torch.distributed (``PartitionedSolid(prob, group=...)``).  Each part's
+elements are ordered interface first (the elements touching a shared node);
+under torch.distributed a step runs the interface elements, gathers the
+shared rows, and sends each neighbouring part the rows of the nodes the two
+share (NCCL send/recv on a communication stream, the reference's
+PAR_INTERFACE_NODE_EXCHANGE with MPI_Isend/Irecv) while the interior
+elements compute; the received rows are added and written back before the
+nodal update.  Steps use the context's sma_step_prologue /
+sma_step_elements(_range) / sma_step_nodes, the same kernels as
 sma_explicit_step without its graphs."""
 import ctypes as C
 
@@ -72,6 +78,61 @@ def layout(prob, parts):
     return node_sets, shared, owner, local
 
 
+def interface_first(prob, elems, shared_mask):
+    """The part's elements with those touching a shared node first (both
+    runs in increasing global order), and the number of interface ones."""
+    touch = shared_mask[prob.lnods[elems]].any(axis=1)
+    return np.concatenate([elems[touch], elems[~touch]]), int(touch.sum())
+
+
+def neighbour_plan(node_sets, local):
+    """Per part k: [(j, positions)] for every other part j sharing nodes with
+    k, positions indexing k's shared rows (ordered by global node id, as
+    ``layout`` lists them) of the nodes k and j share, in increasing global
+    id -- the same nodes in the same order on both sides."""
+    plans = []
+    for k, g in enumerate(node_sets):
+        loc, _ = local[k]
+        gk = g[loc]                                      # global ids of k's shared nodes, increasing
+        plan = []
+        for j, h in enumerate(node_sets):
+            if j == k:
+                continue
+            pos = np.nonzero(np.isin(gk, h, assume_unique=True))[0]
+            if pos.size:
+                plan.append((j, pos.astype(np.int64)))
+        plans.append(plan)
+    return plans
+
+
+def exchange_neighbours(rows, plan, group=None):
+    """The shared rows (n, 3) of this rank summed with its neighbours': the
+    rows of the nodes shared with each neighbour go to it and its rows of
+    the same nodes come back (point-to-point, all posted before any wait),
+    then are added.  NCCL for CUDA tensors; with gloo (host tensors only for
+    point-to-point) CUDA rows are staged through host memory."""
+    import torch
+    import torch.distributed as dist
+    if not plan:
+        return rows.clone()
+    host = rows.is_cuda and dist.get_backend(group) != "nccl"
+    src = rows.cpu() if host else rows
+    ops, bufs = [], []
+    for j, pos in plan:
+        pt = torch.as_tensor(pos, device=src.device)
+        send = src.index_select(0, pt).contiguous()
+        recv = torch.empty_like(send)
+        peer = dist.get_global_rank(group, j) if group is not None else j
+        ops += [dist.P2POp(dist.isend, send, peer, group), dist.P2POp(dist.irecv, recv, peer, group)]
+        bufs.append((pt, recv, send))
+    for r in dist.batch_isend_irecv(ops):
+        r.wait()
+    out = src.clone()
+    for pt, recv, _ in bufs:
+        out.index_add_(0, pt, recv)
+    return out.to(rows.device) if host else out
+
+
 def reduce_shared(rows, slots, nshared, group=None):
     """Sum the rows (n, 3) a rank holds for shared nodes with every other
     rank's rows of the same nodes: each rank places its rows at their slots
@@ -111,8 +172,15 @@ class PartitionedSolid:
         self.parts = partition_elements(prob, nparts)
         self.node_sets, self.shared, owner, self.local = layout(prob, self.parts)
         self.nshared = int(self.shared.size)
+        shared_mask = np.zeros(prob.npoin, bool)
+        shared_mask[self.shared] = True
+        self.n_iface = {}
+        for k in range(nparts):
+            self.parts[k], self.n_iface[k] = interface_first(prob, self.parts[k], shared_mask)
+        self.plan = neighbour_plan(self.node_sets, self.local)
         mine = range(nparts) if group is None else [self.rank]
         self.solids, self.idx, self.slots = {}, {}, {}
+        self._comm = None
         for k in mine:
             dev = device if devices is None else devices[k]
             q, _ = sub_problem(prob, self.parts[k], owner == k)
@@ -158,7 +226,7 @@ class PartitionedSolid:
             with torch.cuda.stream(torch.cuda.ExternalStream(s.stream)):   # ordered with the part's kernels
                 rows = torch.empty((n, 3), dtype=torch.float64, device=self.idx[k].device)
                 self._check(L.sma_gather_residual(s._ctx, n, self.idx[k].data_ptr(), rows.data_ptr()))
-                back = reduce_shared(rows, self.slots[k], self.nshared, self.group).contiguous()
+                back = exchange_neighbours(rows, self.plan[k], self.group).contiguous()
                 self._check(L.sma_scatter_residual(s._ctx, n, self.idx[k].data_ptr(), back.data_ptr()))
                 self._keep = back                     # alive until the stream has used it
             return
@@ -186,11 +254,48 @@ class PartitionedSolid:
             torch.cuda.ExternalStream(s.stream).synchronize()
 
     # -- stepping -----------------------------------------------------------
+    def _step_overlapped(self, nsteps):
+        """Distributed steps: interface elements, shared rows gathered and
+        exchanged with the neighbours on a communication stream while the
+        interior elements compute, sums written back, nodal update."""
+        import torch
+        L = self._lib()
+        k = self.rank
+        s = self.solids[k]
+        idx = self.idx[k]
+        dev = idx.device
+        n, ni, ne = idx.numel(), self.n_iface[k], s.nelem
+        st = torch.cuda.ExternalStream(s.stream)
+        if self._comm is None:
+            self._comm = torch.cuda.Stream(device=dev)
+        comm = self._comm
+        self._check(L.sma_step_prologue(s._ctx))
+        for step in range(nsteps):
+            self._check(L.sma_step_elements_range(s._ctx, 0, ni, 1, 0))
+            with torch.cuda.stream(st):
+                rows = torch.empty((n, 3), dtype=torch.float64, device=dev)
+            self._check(L.sma_gather_residual(s._ctx, n, idx.data_ptr(), rows.data_ptr()))
+            ready = torch.cuda.Event()
+            ready.record(st)
+            comm.wait_event(ready)
+            with torch.cuda.stream(comm):
+                summed = exchange_neighbours(rows, [(j, pos) for j, pos in self.plan[k]], self.group)
+            rows.record_stream(comm)
+            self._check(L.sma_step_elements_range(s._ctx, ni, ne, 0, 1))     # interior, meanwhile
+            done = torch.cuda.Event()
+            done.record(comm)
+            st.wait_event(done)
+            summed.record_stream(st)
+            self._check(L.sma_scatter_residual(s._ctx, n, idx.data_ptr(), summed.data_ptr()))
+            self._check(L.sma_step_nodes(s._ctx, C.c_int32(int(step == nsteps - 1))))
+
     def step(self, nsteps):
         """nsteps explicit steps of the whole mesh (sma_explicit_step's
         sequence on every part, shared residual summed every step)."""
         if nsteps <= 0:
             return
+        if self.group is not None and self.nshared > 0:
+            return self._step_overlapped(nsteps)
         L = self._lib()
         for s in self.solids.values():
             self._check(L.sma_step_prologue(s._ctx))

@@ -19,11 +19,13 @@ elements, tip traction) and ensemble (256 specimens) select the others.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp64] [--scatter atomic|color]
 
---gpus N > 1 (under torchrun): the cantilever and cylinder run one
-independent replica per rank (weak scaling); --workload ensemble shards its
-256 specimens across the ranks, largest first onto the least loaded rank,
-with no exchange (strong scaling).  Either way the time is the maximum over
-ranks of the device time and `value` counts every rank's Gauss points.
+--gpus N > 1 (under torchrun): the cylinder and the cantilever are split
+into N element slabs, one per rank, the interface rows exchanged with the
+neighbouring slabs every step while the interior elements compute (strong
+scaling; --no-partition runs one replica per rank instead); --workload
+ensemble shards its 256 specimens across the ranks, largest first onto the
+least loaded rank, with no exchange (strong scaling).  The time is the
+maximum over ranks of the device time.
 --impl reference times the CPU restatement of the reference path (the
 oracle: the reference is Fortran and cannot be built here) on the host
 cores of rank 0, on a bounded sample of the same workload.
@@ -75,7 +77,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "surrogate"],
+                    help="the timed form: fp32 (FP32 kinematics and law, FP64 return map and integration), "
+                         "fp64, or surrogate (the fp32 form with the learned surrogate in its element loop)")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "color"])
     ap.add_argument("--no-extras", action="store_true", help="skip fp64/e2e/cpu legs")
     ap.add_argument("--div", type=int, default=1, help="coarsen the mesh (tests only)")
@@ -90,11 +94,18 @@ def parse():
     ap.add_argument("--write-profile", metavar="CSV", default=None,
                     help="turn `ncu -i <rep> --page raw --csv` output into the machine-read profile "
                          "summary of this precision/workload (profiles/k_element_<prec>_<workload>.json)")
+    ap.add_argument("--surrogate", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the FP32 form with the learned surrogate (trained first, on the GPU)")
+    ap.add_argument("--surrogate-samples", type=int, default=20_000_000, help="plain-law samples generated")
+    ap.add_argument("--surrogate-epochs", type=int, default=4)
+    ap.add_argument("--surrogate-gate", type=float, default=3.0, help="out-of-envelope score limit")
     ap.add_argument("--block", type=int, default=0, help="threads per element block (0: library default)")
     ap.add_argument("--autotune", action="store_true", help="pick block and scatter by timing candidates")
-    ap.add_argument("--partition", action="store_true",
-                    help="split the one mesh over the ranks (element slabs; the shared nodes' residual "
-                         "summed by an all-reduce every step): strong scaling. Default: a replica per rank")
+    ap.add_argument("--partition", action=argparse.BooleanOptionalAction, default=None,
+                    help="split the one mesh over the ranks (element slabs, interface elements first; the "
+                         "shared nodes' residual exchanged with the neighbouring slabs while the interior "
+                         "elements compute): strong scaling.  Default: on for the cylinder and the "
+                         "cantilever under --gpus N > 1, off at N = 1; the ensemble shards its specimens")
     return ap.parse_args()
 
 
@@ -266,11 +277,13 @@ def per_element_values(prob):
 
 def algorithmic_bytes(prob, precision):
     """Minimum HBM traffic of one element-kernel launch: connectivity, state
-    read + write, the per-element material values and temperature (in the
-    precision's word), one read of coordinates and displacements and one
-    read-modify-write of the residual per node."""
-    s = 4 if precision == "fp32" else 8
-    return prob.nelem * (32 + 2 * 8 * 3 * s + per_element_values(prob) * s) + prob.npoin * (24 + 24 + 48)
+    read + write (with the surrogate also the transformation strain, 6
+    words per Gauss point), the per-element material values and temperature
+    (in the precision's word), one read of coordinates and displacements and
+    one read-modify-write of the residual per node."""
+    s = 8 if precision == "fp64" else 4
+    nstate = 9 if precision == "surrogate" else 3
+    return prob.nelem * (32 + 2 * 8 * nstate * s + per_element_values(prob) * s) + prob.npoin * (24 + 24 + 48)
 
 
 def build_problem(workload, div, rank=0, world=1, layers=0):
@@ -320,6 +333,43 @@ def compare_forms(prob, s32, s64, nsteps):
     if held.any():
         r32, r64 = s32.get("rhsid")[held, 0].sum(), s64.get("rhsid")[held, 0].sum()
         out["far_face_reaction_rel"] = float(abs(r32 - r64) / max(abs(r64), 1e-300))
+    return out
+
+
+def surrogate_leg(args, prob, u0, s64, v64, v32, wsteps, device):
+    """The FP32 form with the learned surrogate in its element loop: trained
+    here by the library's kernels on plain-law paths of the workload's
+    materials, switched on after the same warm-up steps of the plain law
+    from the same start, the same K steps timed; the plain FP64 run (s64,
+    after the same steps) judges its error."""
+    import torch
+    import alya_sma_b200 as sma
+    from alya_sma_b200 import surrogate as S
+    net, info = S.train_for(prob, nsamples=args.surrogate_samples, epochs=args.surrogate_epochs, device=device)
+    g = sma.ExplicitSolid(prob, precision="fp32", scatter=args.scatter, device=device)
+    g.set("displ", u0)
+    g.step(wsteps)
+    g.set_surrogate(net, gate=args.surrogate_gate, xs_tol=1e-3)
+    g.counters(reset=True)
+    st = torch.cuda.ExternalStream(g.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    g.step(args.steps)
+    b.record(st)
+    b.synchronize()
+    ngp = prob.nelem * 8
+    ms = a.elapsed_time(b)
+    v = ngp * args.steps / (ms / 1e3)
+    c = g.counters()
+    out = {"value": v, "unit": "GP-updates/s", "ms_per_step": ms / args.steps,
+           "speedup_vs_plain_fp64": round(v / v64, 3), "speedup_vs_fp32_form": round(v / v32, 3),
+           "fallback_fraction": c["sur_fallback"] / (ngp * args.steps),
+           "out_of_envelope_fraction": c["sur_ood"] / (ngp * args.steps),
+           "return_map_fraction": c["nr_active"] / (ngp * args.steps),
+           "tensor_core_status": g.surrogate_status(), "gate": args.surrogate_gate,
+           "network": "14 -> 64x4 (SiLU) -> 13, BF16 tcgen05.mma with FP32 accumulation in TMEM",
+           "training": info, "error_vs_fp64": compare_forms(prob, g, s64, wsteps + args.steps)}
+    g.close()
     return out
 
 
@@ -383,16 +433,20 @@ def run_reference(args):
 
 def run_partitioned(args, rank, world, local):
     """--partition: every rank builds the whole mesh, keeps its element slab
-    and steps it with the others, the shared nodes' residual summed between
-    the element loop and the nodal update (NCCL under torchrun).  value =
-    the mesh's Gauss points (each counted once) x K / the slowest rank's
-    time.  The per-step events of a second window time the part's element
-    launch, the exchange and the nodal launch."""
+    and steps it with the others: interface elements, the shared rows sent
+    to and received from the neighbouring slabs (NCCL send/recv under
+    torchrun) while the interior elements compute, the sums written back,
+    the nodal update.  value = the mesh's Gauss points (each counted once)
+    x K / the slowest rank's time.  The per-step events of a second window
+    time the part's element launch, the (unoverlapped) exchange and the
+    nodal launch."""
     import torch
     import alya_sma_b200 as sma
     from alya_sma_b200 import dist as D
     from alya_sma_b200 import partition as PT
     from alya_sma_b200 import problem as P
+    if args.precision == "surrogate":
+        raise SystemExit("--partition runs the fp32 or fp64 form")
     prob = build_problem(args.workload, args.div, layers=args.layers)
     group = torch.distributed.group.WORLD if world > 1 else None
     ps = PT.PartitionedSolid(prob, nparts=1, precision=args.precision, scatter=args.scatter, device=local,
@@ -441,6 +495,28 @@ def run_partitioned(args, rank, world, local):
     nd_ms = sum(e[2].elapsed_time(e[3]) for e in ev) / args.steps
     k = rank if group is not None else 0
     q, _ = PT.sub_problem(prob, ps.parts[k], np.ones(prob.npoin, bool))
+    # e2e: every rank's element-loop C-ABI call on its slab with pinned host
+    # buffers (its displacement in, its residual out), the job's Gauss points
+    # over the slowest rank's time
+    npart = part.npoin
+    hd = torch.zeros((npart, 3), dtype=torch.float64).pin_memory()
+    hr = torch.zeros((npart, 3), dtype=torch.float64).pin_memory()
+    hd.copy_(torch.from_numpy(part.get("displ")))
+    dnp, rnp = hd.numpy(), hr.numpy()
+    for _ in range(3):
+        sma._check(L.sma_assemble(part._ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
+        part.end_step()
+    ke = max(10, args.steps // 20)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        sma._check(L.sma_assemble(part._ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
+        part.end_step()
+    te = D.max_over_ranks(time.perf_counter() - t0, "cuda")
+    e2e = {"value": ngp * ke / te, "unit": "GP-updates/s", "h2d_bytes_per_step": 3 * npart * 8,
+           "d2h_bytes_per_step": 3 * npart * 8,
+           "boundary": "sma_assemble on each rank's slab (host displ in, host rhsid out), slowest rank's time"}
     alg = algorithmic_bytes(q, args.precision)
     peak, peak_kind = measured_peaks()
     achieved = alg / (el_ms / 1e3) / 1e9
@@ -462,10 +538,9 @@ def run_partitioned(args, rank, world, local):
                            "npoin": prob.npoin, "gauss_points": ngp, "precision": args.precision,
                            "scatter": args.scatter, "prestrain": args.prestrain,
                            "parallelism": f"one mesh in {world} element slabs, {ps.nshared} shared nodes "
-                                          "summed every step"},
-                "roofline": roofline, "gpu_launches": launches, "clocks": ck,
-                "e2e": {"value": None, "unit": "GP-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
-                        "boundary": "not measured in --partition mode (the default mode measures sma_assemble)"}}
+                                          "exchanged with the neighbouring slabs every step, overlapped with the "
+                                          "interior elements"},
+                "roofline": roofline, "gpu_launches": launches, "clocks": ck, "e2e": e2e}
         print(json.dumps(line))
     ps.close()
     if world > 1:
@@ -493,6 +568,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+    if args.partition is None:
+        args.partition = world > 1 and args.workload != "ensemble"
     if args.partition:
         return run_partitioned(args, rank, world, local)
     prob = build_problem(args.workload, args.div, rank, world, layers=args.layers)
@@ -509,11 +586,22 @@ def main():
     else:
         variant = "auto"
     args.scatter = scatter
-    solid = sma.ExplicitSolid(prob, precision=args.precision, scatter=scatter, block=block,
+    # --precision surrogate: the FP32 form with the learned surrogate in its
+    # element loop is the timed form (trained first; the warm-up runs the
+    # plain law, as the surrogate leg of the default run does)
+    net, sur_info = None, None
+    prec = "fp32" if args.precision == "surrogate" else args.precision
+    if args.precision == "surrogate":
+        from alya_sma_b200 import surrogate as S
+        net, sur_info = S.train_for(prob, nsamples=args.surrogate_samples, epochs=args.surrogate_epochs,
+                                    device=local)
+    solid = sma.ExplicitSolid(prob, precision=prec, scatter=scatter, block=block,
                               device=local, variant=variant)
     solid.set("displ", u0)
     stream = torch.cuda.ExternalStream(solid.stream)
     solid.step(max(3, args.warmup))
+    if net is not None:
+        solid.set_surrogate(net, gate=args.surrogate_gate, xs_tol=1e-3)
 
     def barrier():
         if world > 1:
@@ -547,6 +635,10 @@ def main():
     physics = {"gauss_points_in_return_map_per_step": round(cnt["nr_active"] / args.steps),
                "return_map_failures": cnt["nr_failed"], "det_F_nonpositive": cnt["neg_det"],
                "nonfinite": cnt["nonfinite"]}
+    if net is not None:
+        physics["surrogate_fallback_fraction"] = cnt["sur_fallback"] / (ngp * args.steps)
+        physics["surrogate_out_of_envelope_fraction"] = cnt["sur_ood"] / (ngp * args.steps)
+        physics["surrogate_training"] = sur_info
     ngp_all = world * ngp                                      # replicas: the same mesh per rank
     from alya_sma_b200 import dist as D                       # (identity on one rank)
     if world > 1:
@@ -561,6 +653,8 @@ def main():
     solid.load(ckpt)
     os.remove(ckpt)
     os.rmdir(os.path.dirname(ckpt))
+    if net is not None:                        # eps_tr derived again from the window's start
+        solid.set_surrogate(net, gate=args.surrogate_gate, xs_tol=1e-3)
     solid.set_timing(True)
     solid.step(args.steps)
     tm = solid.timers()
@@ -594,7 +688,7 @@ def main():
                              "frac": round(rate / peak_i, 4)}
 
     extras = {}
-    if not args.no_extras and rank == 0 and args.precision != "fp64":
+    if not args.no_extras and rank == 0 and args.precision == "fp32":
         # the plain FP64 form: the same steps from the same start, its K
         # steps timed like the FP32 window; then both forms compared
         wsteps = max(3, args.warmup)
@@ -612,6 +706,8 @@ def main():
                                 "ms_per_step": a.elapsed_time(b) / args.steps}
         extras["speedup_vs_plain_fp64"] = round(value / world / v64, 3)
         extras["error_vs_fp64"] = compare_forms(prob, solid, s64, wsteps + args.steps)
+        if args.surrogate:
+            extras["surrogate"] = surrogate_leg(args, prob, u0, s64, v64, value / world, wsteps, local)
         s64.close()
     if not args.no_extras:
         # e2e on every rank: the element-loop C-ABI call with pinned host
@@ -647,7 +743,7 @@ def main():
                 "unit": "GP-updates/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "strong" if sharded else "weak", "vs_baseline": None,
-                "dtype": "f32+f64" if args.precision == "fp32" else "f64",
+                "dtype": {"fp32": "f32+f64", "fp64": "f64", "surrogate": "bf16+f32+f64"}[args.precision],
                 "data": "synthetic",
                 "config": {"workload": workload_name(args.workload, args.div), "nelem": nelem, "npoin": prob.npoin,
                            "gauss_points": ngp_all, "precision": args.precision,

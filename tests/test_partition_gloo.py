@@ -91,3 +91,74 @@ def test_shared_rows_summed_over_gloo_ranks():
             who = [k for k in range(world) if g in set(node_sets[k].tolist())]
             expect = [sum((k + 1) * g + c for k in who) for c in range(3)]
             assert np.allclose(summed[i], expect)
+
+
+def test_interface_elements_come_first():
+    bar = P.bar_40x4x4(nsteps=10)
+    parts = PT.partition_elements(bar, 3)
+    _, shared, _, _ = PT.layout(bar, parts)
+    mask = np.zeros(bar.npoin, bool)
+    mask[shared] = True
+    for e in parts:
+        order, ni = PT.interface_first(bar, e, mask)
+        assert np.array_equal(np.sort(order), e)                            # same elements
+        touch = mask[bar.lnods[order]].any(axis=1)
+        assert touch[:ni].all() and not touch[ni:].any() and ni > 0
+
+
+def _mixed_parts(bar, world):
+    """A partition with nodes held by up to four parts: the first element
+    layer dealt round robin over the ranks, the rest in slabs."""
+    first = np.arange(16)
+    rest = PT.partition_elements(bar, world)
+    parts = []
+    for k in range(world):
+        mine = np.concatenate([first[first % world == k], np.setdiff1d(rest[k], first)])
+        parts.append(np.sort(mine))
+    return parts
+
+
+def _neighbour_worker(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as tdist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    tdist.init_process_group("gloo", rank=rank, world_size=world,
+                             timeout=datetime.timedelta(seconds=60))
+    bar = P.bar_40x4x4(nsteps=10)
+    parts = _mixed_parts(bar, world)
+    node_sets, shared, owner, local = PT.layout(bar, parts)
+    plan = PT.neighbour_plan(node_sets, local)
+    loc, sl = local[rank]
+    gid = node_sets[rank][loc]
+    rows = torch.as_tensor(np.stack([np.sin(gid * (rank + 2.0)) + c for c in range(3)], axis=1),
+                           dtype=torch.float64)
+    by_neighbours = PT.exchange_neighbours(rows, plan[rank]).numpy()
+    by_allreduce = PT.reduce_shared(rows, torch.as_tensor(sl), shared.size).numpy()
+    out[rank] = (by_neighbours, by_allreduce, len(plan[rank]))
+    tdist.barrier()
+    tdist.destroy_process_group()
+
+
+def test_neighbour_exchange_equals_the_all_reduce():
+    """The per-step sum of shared rows by point-to-point exchange with the
+    neighbouring parts only (what a partitioned run does, overlapped with
+    its interior elements) equals the all-reduce over every shared node,
+    with nodes held by up to four parts."""
+    world = 4
+    port = _free_port()
+    with mp.get_context("spawn").Manager() as man:
+        out = man.dict()
+        mp.spawn(_neighbour_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    bar = P.bar_40x4x4(nsteps=10)
+    node_sets, shared, _, _ = PT.layout(bar, _mixed_parts(bar, world))
+    cnt = np.zeros(bar.npoin, int)
+    for g in node_sets:
+        cnt[g] += 1
+    assert cnt.max() >= 3                                   # some nodes held by three or more parts
+    for r in range(world):
+        nb, ar, nplan = res[r]
+        assert nplan >= 1
+        assert np.allclose(nb, ar, rtol=0, atol=1e-12)
