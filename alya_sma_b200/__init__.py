@@ -303,18 +303,20 @@ class ExplicitSolid:
         _check(lib().sma_get_witness(self._ctx, _p(out), C.byref(n)))
         return out[: n.value]
 
-    def set_surrogate(self, net, gate=3.0, xs_tol=1e-3, enable=True):
+    def set_surrogate(self, net, gate=3.0, xs_tol=1e-3, f_margin=10.0, period=64, enable=True):
         """The learned surrogate (alya_sma_b200.surrogate.Surrogate) in the
         element loop of this FP32 context (sma_set_surrogate), or back to the
         plain law with enable=False."""
         L = lib()
-        L.sma_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int32]
+        L.sma_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                        C.c_int32, C.c_int32]
         if not enable:
-            _check(L.sma_set_surrogate(self._ctx, None, None, 1.0, 0.0, 0))
+            _check(L.sma_set_surrogate(self._ctx, None, None, 1.0, 0.0, 0.0, 1, 0))
             return
         w = np.ascontiguousarray(net.params(), dtype=np.float32)
         st = net.stats_host
-        _check(L.sma_set_surrogate(self._ctx, w.ctypes.data, C.addressof(st), float(gate), float(xs_tol), 1))
+        _check(L.sma_set_surrogate(self._ctx, w.ctypes.data, C.addressof(st), float(gate), float(xs_tol),
+                                   float(f_margin), int(period), 1))
         self._sur_keep = (w, st)
 
     def surrogate_status(self):
@@ -323,6 +325,16 @@ class ExplicitSolid:
         L.sma_surrogate_status.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
         _check(L.sma_surrogate_status(self._ctx, C.byref(s)))
         return int(s.value)
+
+    def set_launch_plan(self, ends, blocks):
+        """Element ranges [ends[r-1], ends[r]) launched with blocks[r] threads
+        per block (sma_set_launch_plan); empty lists return to one launch."""
+        L = lib()
+        L.sma_set_launch_plan.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        e = np.ascontiguousarray(ends, dtype=np.int32)
+        b = np.ascontiguousarray(blocks, dtype=np.int32)
+        _check(L.sma_set_launch_plan(self._ctx, int(e.size), _p(e) if e.size else None,
+                                     _p(b) if b.size else None))
 
     def critical_dt(self):
         d = C.c_double()

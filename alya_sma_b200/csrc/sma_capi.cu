@@ -247,12 +247,16 @@ struct sma_ctx {
   void* d_matx = nullptr;                  // compact per-element records (T [nelem][MATX]) or null
   bool compact = false;                    // element kernel reads d_matx instead of d_mats
   // learned surrogate (FP32 form): weight image, statistics, eps_tr ping-pong
+  // per-range element blocks (sma_set_launch_plan): plan_end[r] ends range r
+  std::vector<int32_t> plan_end, plan_block;
   bool sur = false;
   unsigned char* d_sur_img = nullptr;
   sur::SurStats* d_sur_stats = nullptr;
   float* d_etr[2] = {nullptr, nullptr};    // [6][sst] per state buffer
+  __half* d_rcache = nullptr;              // the network's held residual, [6][sst] FP16
+  int sur_period = 64;
   int* d_sur_ctr = nullptr;                // [0] tile counter, [1] status
-  float sur_gate = 3.0f, sur_xs_tol = 1e-3f;
+  float sur_gate = 3.0f, sur_xs_tol = 1e-3f, sur_margin = 10.0f;
   int sur_grid = 0;
   void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
   int cur = 0;                             // state buffer holding TIME_N
@@ -457,6 +461,10 @@ int32_t launch_sur_range(sma_ctx* c, int beg, int end, bool advance, bool steppi
   s.status = c->d_sur_ctr + 1;
   s.gate = c->sur_gate;
   s.xs_tol = c->sur_xs_tol;
+  s.f_margin = c->sur_margin;
+  s.rcache = c->d_rcache;
+  s.clock = c->d_ts;
+  s.period = c->sur_period;
   CU(cudaMemsetAsync(c->d_sur_ctr, 0, sizeof(int), c->stream));
   const int64_t ntiles = ceil_div(end - beg, sur::SUR_EPB);
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, c->sur_grid);
@@ -464,6 +472,28 @@ int32_t launch_sur_range(sma_ctx* c, int beg, int end, bool advance, bool steppi
   if (c->compact) sur::k_element_sur<true><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
   else sur::k_element_sur<false><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
   c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+// the element loop by the launch plan: range r with its own block size (the
+// one-tile kernel, narrow or wide instance by block)
+template <typename T>
+int32_t launch_plan_t(sma_ctx* c, bool advance) {
+  int beg = 0;
+  const int saved = c->block;
+  for (size_t r = 0; r < c->plan_end.size(); ++r) {
+    const int end = c->plan_end[r];
+    if (end > beg) {
+      c->block = c->plan_block[r];
+      ElemArgs<T> a = elem_args<T>(c, beg, end, advance && beg == 0, advance);
+      const unsigned grid = (unsigned)ceil_div(end - beg, c->block / 8);
+      elem_kernel<T>(c)<<<grid, c->block, elem_smem<T>(c), c->stream>>>(a);
+      c->launches++;
+    }
+    beg = end;
+  }
+  c->block = saved;
   CU(cudaGetLastError());
   return SMA_OK;
 }
@@ -478,6 +508,10 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
       c->last_in = c->cur;
       return launch_sur_range(c, 0, c->nelem, advance, advance);
     }
+  }
+  if (!c->plan_end.empty()) {
+    c->last_in = c->cur;
+    return launch_plan_t<T>(c, advance);
   }
   c->last_in = c->cur;
   const ElemKernel<T> kern = elem_kernel<T>(c);
@@ -777,8 +811,13 @@ int32_t build_graphs(sma_ctx* c, int chunk) {
 }
 
 int64_t kernels_per_step(const sma_ctx* c) {
-  return (int64_t)(c->cptr.size() - 1) + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0) +
-         (c->energy && c->damp ? 1 : 0);
+  int64_t elem = (int64_t)(c->cptr.size() - 1);
+  if (!c->sur && !c->plan_end.empty()) {
+    elem = 0;
+    for (size_t r = 0; r < c->plan_end.size(); ++r)
+      elem += c->plan_end[r] > (r ? c->plan_end[r - 1] : 0);
+  }
+  return elem + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0) + (c->energy && c->damp ? 1 : 0);
 }
 
 template <typename T>
@@ -806,7 +845,7 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->l2_window) cudaCtxResetPersistingL2Cache();   // release the lines this context pinned
   void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_nodal, c->d_matx, c->d_sur_img, c->d_sur_stats,
-                  c->d_etr[0], c->d_etr[1], c->d_sur_ctr,
+                  c->d_etr[0], c->d_etr[1], c->d_sur_ctr, c->d_rcache,
                   c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
@@ -1993,7 +2032,7 @@ extern "C" int32_t sma_noalloc_counters(sma_counters* out, void* stream) {
 // the learned surrogate in the element loop
 // ---------------------------------------------------------------------------
 extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_sur_stats* stats, double gate,
-                                     double xs_tol, int32_t enable) {
+                                     double xs_tol, double f_margin, int32_t period, int32_t enable) {
   if (!c) return fail(SMA_ERR_ARG, "NULL context");
   CU(cudaSetDevice(c->dev));
   if (!enable) {
@@ -2007,7 +2046,8 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   if (c->damp) return fail(SMA_ERR_ARG, "the surrogate element loop has no Rayleigh damping");
   if (c->d_lmate && !c->compact)
     return fail(SMA_ERR_ARG, "per-element materials need compact records for the surrogate");
-  if (!(gate > 0.0) || !(xs_tol >= 0.0)) return fail(SMA_ERR_ARG, "gate > 0, xs_tol >= 0");
+  if (!(gate > 0.0) || !(xs_tol >= 0.0) || !(f_margin >= 0.0) || period < 1)
+    return fail(SMA_ERR_ARG, "gate > 0, xs_tol >= 0, f_margin >= 0, period >= 1");
   for (int k = 0; k < SMA_SUR_NPARAM; ++k)
     if (!std::isfinite(params[k])) return fail(SMA_ERR_ARG, "non-finite surrogate parameter");
   int32_t rc;
@@ -2017,6 +2057,7 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
     if ((rc = dalloc(&c->d_sur_ctr, 2 * sizeof(int)))) return rc;
     for (int b = 0; b < 2; ++b)
       if ((rc = dalloc(&c->d_etr[b], 6 * (size_t)c->sst * sizeof(float)))) return rc;
+    if ((rc = dalloc(&c->d_rcache, 6 * (size_t)c->sst * sizeof(__half)))) return rc;
     CU(cudaFuncSetAttribute(sur::k_element_sur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)sur::sur_elem_smem_bytes()));
     CU(cudaFuncSetAttribute(sur::k_element_sur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2033,6 +2074,7 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   sur::k_sur_pack_image<<<(sur::HID * sur::HID + 255) / 256, 256, 0, c->stream>>>(d_w, c->d_sur_img);
   CU(cudaMemcpyAsync(c->d_sur_stats, stats, sizeof(sur::SurStats), cudaMemcpyHostToDevice, c->stream));
   CU(cudaMemsetAsync(c->d_sur_ctr, 0, 2 * sizeof(int), c->stream));
+  CU(cudaMemsetAsync(c->d_rcache, 0xff, 6 * (size_t)c->sst * sizeof(__half), c->stream));   // NaN: none held
   // eps_tr of the TIME_N state at the current displacement
   {
     ElemArgs<float> a = elem_args<float>(c, 0, c->nelem, false, false);
@@ -2051,6 +2093,8 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   c->sur_grid = c->nsm * per_sm;
   c->sur_gate = (float)gate;
   c->sur_xs_tol = (float)xs_tol;
+  c->sur_margin = (float)f_margin;
+  c->sur_period = period;
   destroy_graphs(c);
   c->sur = true;
   return SMA_OK;
@@ -2067,5 +2111,36 @@ extern "C" int32_t sma_surrogate_status(sma_ctx* c, int32_t* status) {
   CU(cudaSetDevice(c->dev));
   CU(cudaMemcpyAsync(status, c->d_sur_ctr + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
+  return SMA_OK;
+}
+
+// Launch plan of the element loop: nrange element ranges [end[r-1], end[r])
+// (end increasing, the last = nelem) each launched with its own threads per
+// block -- the ensemble's specimen-size buckets, tuned one by one.  One-tile
+// kernel with the atomic scatter only; nrange = 0 returns to one launch.
+extern "C" int32_t sma_set_launch_plan(sma_ctx* c, int32_t nrange, const int32_t* end, const int32_t* block) {
+  if (!c) return fail(SMA_ERR_ARG, "NULL context");
+  if (nrange < 0) return fail(SMA_ERR_ARG, "nrange < 0");
+  if (nrange == 0) {
+    c->plan_end.clear();
+    c->plan_block.clear();
+    destroy_graphs(c);
+    return SMA_OK;
+  }
+  if (!end || !block) return fail(SMA_ERR_ARG, "NULL argument");
+  if (c->scatter != SMA_SCATTER_ATOMIC || c->variant != SMA_VARIANT_PLAIN)
+    return fail(SMA_ERR_ARG, "launch plans need the atomic scatter and the one-tile kernel");
+  int prev = 0;
+  for (int r = 0; r < nrange; ++r) {
+    if (end[r] < prev || end[r] > c->nelem) return fail(SMA_ERR_ARG, "plan ends must increase within nelem");
+    if (block[r] % 32 != 0 || block[r] < 32 || block[r] > 256)
+      return fail(SMA_ERR_ARG, "plan blocks must be multiples of 32 in [32, 256]");
+    prev = end[r];
+  }
+  if (end[nrange - 1] != c->nelem) return fail(SMA_ERR_ARG, "the last plan range must end at nelem");
+  CU(cudaSetDevice(c->dev));
+  c->plan_end.assign(end, end + nrange);
+  c->plan_block.assign(block, block + nrange);
+  destroy_graphs(c);
   return SMA_OK;
 }

@@ -14,16 +14,18 @@
 //            transformation strain eL xS D, D the unit deviatoric direction
 //            of ln U, 6), temperature, xS of the previous step
 //   outputs  (S - S_p) / E(xS0) (6): the second Piola-Kirchhoff stress less
-//            its analytic part S_p (stress_predictor: the law's elastic
-//            response on a second-order logarithmic strain), over the
-//            Reuss modulus, so the network carries only the higher-order
-//            remainder; xS - xS0; eps_tr - eps_tr0 (6)
+//            its analytic part S_p (analytic_part: the law's elastic
+//            response on a third-order logarithmic strain, the
+//            transformation strain turned onto the current direction), over
+//            the Reuss modulus, so the network carries only the remainder;
+//            xS - xS0; eps_tr - eps_tr_p (6), eps_tr_p the turned eps_tr0
 // Inputs and outputs are normalised per feature by the training set's mean
 // and standard deviation (SurStats).  Weights are BF16 with FP32
 // accumulation on the tensor cores; biases and the epilogue are FP32.
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "sma_law.cuh"
 
@@ -48,6 +50,7 @@ static_assert(NPARAM == 14608, "parameter layout");
 struct SurStats {
   float mu_x[NIN], sd_x[NIN], mu_y[NOUT], sd_y[NOUT];
   float Linv[NIN * NIN];
+  float lo_x[NIN], hi_x[NIN];   // the training inputs' range: outside it is out of the envelope
 };
 
 // ---------------------------------------------------------------------------
@@ -93,30 +96,52 @@ __device__ __forceinline__ void lin_elastic(double kK, double kG, const T* e, T*
   s[5] = mu2 * e[5];
 }
 
-// The analytic part of the stress, S_p / E(xS0), from a second-order
-// logarithmic strain ln U ~ E - E^2 (exact to O(E^3); E the Green-Lagrange
-// strain, C = I + 2E): T_p = kK (tr h - 3 alpha |eps_tr0|) I
-// + 2 kG (dev h - eps_tr0), S_p = sym(C^-1 T_p) -- the law's elastic
-// response (sld_stress_model_160.f90:487-491) with eps_tr0 = eL xS0 D as
-// its transformation strain, so the network carries only the higher-order
-// remainder and the turn of D within the step.
+// The analytic part of the response.  h = E - E^2 + 4/3 E^3 is ln U to
+// O(E^4) (E the Green-Lagrange strain, C = I + 2E).  The law's transformation
+// strain always lies along the current deviatoric direction (eL xS D,
+// sld_stress_model_160.f90:487-491), so the previous step's eps_tr0 is turned
+// onto dev h: eps_tr = |eps_tr0| dev h / |dev h|.  Then
+// T_p = kK (tr h - 3 alpha |eps_tr|) I + 2 kG (dev h - eps_tr) and
+// S_p = sym(C^-1 T_p) -- the law's elastic response over E(xS0), so the
+// network carries only the O(E^4) remainder.
 template <typename T>
-__device__ __forceinline__ void stress_predictor(double kK, double kG, double alfa, const T* E, const T* etr,
-                                                 T* Sp) {
-  // h = E - E^2
-  const T e2_00 = E[0] * E[0] + E[3] * E[3] + E[5] * E[5];
-  const T e2_11 = E[3] * E[3] + E[1] * E[1] + E[4] * E[4];
-  const T e2_22 = E[5] * E[5] + E[4] * E[4] + E[2] * E[2];
-  const T e2_01 = E[0] * E[3] + E[3] * E[1] + E[5] * E[4];
-  const T e2_12 = E[3] * E[5] + E[1] * E[4] + E[4] * E[2];
-  const T e2_02 = E[0] * E[5] + E[3] * E[4] + E[5] * E[2];
-  const T h[6] = {E[0] - e2_00, E[1] - e2_11, E[2] - e2_22, E[3] - e2_01, E[4] - e2_12, E[5] - e2_02};
-  const T tr = h[0] + h[1] + h[2];
-  const T ntr = sqrt(etr[0] * etr[0] + etr[1] * etr[1] + etr[2] * etr[2] +
-                     T(2) * (etr[3] * etr[3] + etr[4] * etr[4] + etr[5] * etr[5]));
-  const T pv = (T)kK * (tr - T(3) * (T)alfa * ntr), g2 = T(2) * (T)kG, t3 = tr * (T(1) / T(3));
-  const T Tp[6] = {pv + g2 * (h[0] - t3 - etr[0]), pv + g2 * (h[1] - t3 - etr[1]), pv + g2 * (h[2] - t3 - etr[2]),
-                   g2 * (h[3] - etr[3]), g2 * (h[4] - etr[4]), g2 * (h[5] - etr[5])};
+__device__ __forceinline__ void analytic_part(double kK, double kG, double alfa, const T* E, const T* etr0,
+                                              T* Sp, T* etr) {
+  // E^2 and E^3 (symmetric products, xx yy zz xy yz xz)
+  T q[6];
+  q[0] = E[0] * E[0] + E[3] * E[3] + E[5] * E[5];
+  q[1] = E[3] * E[3] + E[1] * E[1] + E[4] * E[4];
+  q[2] = E[5] * E[5] + E[4] * E[4] + E[2] * E[2];
+  q[3] = E[0] * E[3] + E[3] * E[1] + E[5] * E[4];
+  q[4] = E[3] * E[5] + E[1] * E[4] + E[4] * E[2];
+  q[5] = E[0] * E[5] + E[3] * E[4] + E[5] * E[2];
+  T c[6];
+  c[0] = q[0] * E[0] + q[3] * E[3] + q[5] * E[5];
+  c[1] = q[3] * E[3] + q[1] * E[1] + q[4] * E[4];
+  c[2] = q[5] * E[5] + q[4] * E[4] + q[2] * E[2];
+  c[3] = q[0] * E[3] + q[3] * E[1] + q[5] * E[4];
+  c[4] = q[3] * E[5] + q[1] * E[4] + q[4] * E[2];
+  c[5] = q[0] * E[5] + q[3] * E[4] + q[5] * E[2];
+  const T f3 = T(4) / T(3);
+  T h[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) h[k] = E[k] - q[k] + f3 * c[k];
+  const T tr = h[0] + h[1] + h[2], t3 = tr * (T(1) / T(3));
+  const T dh[6] = {h[0] - t3, h[1] - t3, h[2] - t3, h[3], h[4], h[5]};
+  const T ndh = sqrt(dh[0] * dh[0] + dh[1] * dh[1] + dh[2] * dh[2] + T(2) * (dh[3] * dh[3] + dh[4] * dh[4] + dh[5] * dh[5]));
+  const T ntr = sqrt(etr0[0] * etr0[0] + etr0[1] * etr0[1] + etr0[2] * etr0[2] +
+                     T(2) * (etr0[3] * etr0[3] + etr0[4] * etr0[4] + etr0[5] * etr0[5]));
+  if (ndh > T(1e-12)) {
+    const T sc = ntr / ndh;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) etr[k] = sc * dh[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) etr[k] = etr0[k];
+  }
+  const T pv = (T)kK * (tr - T(3) * (T)alfa * ntr), g2 = T(2) * (T)kG;
+  const T Tp[6] = {pv + g2 * (dh[0] - etr[0]), pv + g2 * (dh[1] - etr[1]), pv + g2 * (dh[2] - etr[2]),
+                   g2 * (dh[3] - etr[3]), g2 * (dh[4] - etr[4]), g2 * (dh[5] - etr[5])};
   const T Cm[6] = {T(1) + T(2) * E[0], T(1) + T(2) * E[1], T(1) + T(2) * E[2], T(2) * E[3], T(2) * E[4],
                    T(2) * E[5]};
   T Ci[6];
@@ -283,9 +308,9 @@ static __global__ void k_sur_generate(GenArgs g) {
     // sample
     float* xo = g.x + (path * g.nstep + s) * NIN;
     float* yo = g.y + (path * g.nstep + s) * NOUT;
-    double E[6], sl[6];
+    double E[6], sl[6], er[6];
     for (int c = 0; c < 6; ++c) E[c] = 0.5 * A[c];
-    stress_predictor<double>(m.kK, m.kG, m.alfa, E, etr, sl);
+    analytic_part<double>(m.kK, m.kG, m.alfa, E, etr, sl, er);
     for (int c = 0; c < 6; ++c) {
       xo[c] = (float)E[c];
       xo[6 + c] = (float)etr[c];
@@ -294,7 +319,7 @@ static __global__ void k_sur_generate(GenArgs g) {
     xo[12] = (float)tmp;
     xo[13] = (float)xS0;
     yo[6] = (float)(xSm - xS0);
-    for (int c = 0; c < 6; ++c) yo[7 + c] = (float)(m.eL * xSm * D[c] - etr[c]);
+    for (int c = 0; c < 6; ++c) yo[7 + c] = (float)(m.eL * xSm * D[c] - er[c]);
     }
   }
 }
@@ -901,12 +926,19 @@ __device__ __forceinline__ bool mlp_tile(MlpSmem& s, const float* xh, float* yh)
   return true;
 }
 
-// normalised inputs and the out-of-envelope score of one raw input row
+// normalised inputs and the out-of-envelope score of one raw input row:
+// the Mahalanobis distance per dimension, or +inf if an input lies outside
+// the training inputs' range (a single feature's excursion, which the
+// distance averages over 14 dimensions)
 __device__ __forceinline__ float normalise(const SurStats& st, const float* x, float* xh) {
+  bool out = false;
 #pragma unroll
-  for (int c = 0; c < NIN; ++c) xh[c] = (x[c] - st.mu_x[c]) / st.sd_x[c];
+  for (int c = 0; c < NIN; ++c) {
+    xh[c] = (x[c] - st.mu_x[c]) / st.sd_x[c];
+    out |= !(x[c] >= st.lo_x[c] && x[c] <= st.hi_x[c]);
+  }
   xh[14] = xh[15] = 0.f;
-  float d2 = 0.f;
+  float d2 = out ? __int_as_float(0x7f800000) : 0.f;
 #pragma unroll
   for (int i = 0; i < NIN; ++i) {
     float u = 0.f;

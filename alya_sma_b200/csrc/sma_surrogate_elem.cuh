@@ -6,21 +6,26 @@
 // Per Gauss point (lane = Gauss point, 8 lanes per element, 16 elements =
 // 128 Gauss points = one M = 128 tile per block):
 //   1. gather, kinematics (as k_element), E = (C - I)/2;
-//   2. the network on the block's 128 points (tcgen05.mma into TMEM);
-//   3. S = E(xS0) y_S + S_p (stress_predictor), the rotated-back Kirchhoff stress
+//   2. the network on the block's 128 points (tcgen05.mma into TMEM) every
+//      `period` steps per tile (staggered) or when a point has no residual,
+//      the residual held in between (FP16 per Gauss point);
+//   3. S = E(xS0) (y_S + S_p) (analytic_part: eps_tr turned onto the current
+//      strain direction, as the law keeps it), the rotated-back Kirchhoff stress
 //      T = sym(C S) and from it the law's loading functions
-//      F = |dev T| + 3 alpha tr(T)/3 - C T_K (sld_stress_model_160.f90:
-//      513-537 with beta = 1, |dev T| = 2G (|e| - eL xS0));
-//   4. gates: the out-of-envelope score above its limit, the law's
-//      activation test on those loading functions (:351-374: a point about
-//      to transform needs the return map), or a network xS increment above
+//      F = +-|dev T| + 3 alpha tr(T)/3 - C T_K (sld_stress_model_160.f90:
+//      513-537 with beta = 1: +-|dev T| = 2G (|e| - eL xS0), negative below
+//      the transformation strain);
+//   4. gates: the out-of-envelope score above its limit, loading functions
+//      within f_margin of a transformation start (F_AS > Rs_AS - margin with
+//      xS0 < 1, F_SA < Rs_SA + margin with xS0 > 0: the law's activation test,
+//      :351-374, needs the exact F there), or a network xS increment above
 //      its tolerance on a point the law leaves inactive (its residual
 //      (F - Rf) dh + H (F - F0)(1 - xS) is then not zero) -> the plain law
 //      (material frame, FP32 kinematics, FP64 return map) for that point;
 //   5. tau = F S F^T and the element forces as k_element (tile_forces).
-// Accepted points keep xS0 and eps_tr0 and store the loading functions of
-// the predicted stress as (F_AS, F_SA); fallback points store the law's
-// (xS, F_AS, F_SA) and eps_tr = eL xS D.
+// Accepted points keep xS0, turn eps_tr onto the current direction and
+// store the loading functions of the predicted stress as (F_AS, F_SA);
+// fallback points store the law's (xS, F_AS, F_SA) and eps_tr = eL xS D.
 #pragma once
 
 #include "sma_kernels.cuh"
@@ -34,10 +39,14 @@ struct SurElemArgs {
   const SurStats* stats;
   const float* etr_old;       // eps_tr at TIME_N, SoA [6][sst]
   float* etr_new;             // eps_tr at ITER_K
+  __half* rcache;             // the network's stress residual per Gauss point, SoA [6][sst] (NaN: none)
+  const StepTime* clock;      // the step's time (its index picks the tiles that refresh)
   int* tile_ctr;              // next tile (zeroed before the launch)
   int* status;                // set to 1 if a wait for the tensor cores ran out
   float gate;                 // out-of-envelope score limit
   float xs_tol;               // network xS increment allowed on an inactive point
+  float f_margin;             // distance from the transformation surfaces (loading-function units)
+  int period;                 // steps between two evaluations of the network on a tile
 };
 
 constexpr int SUR_BLOCK = 128, SUR_EPB = SUR_BLOCK / 8;
@@ -105,38 +114,57 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
     else tmp = a.tempe ? __ldg(a.tempe + ec) : 0.0;
     float A2[6];                                                 // C - I = 2E
     green_2E<float>(H, A2);
-    // ---- the network on the block's 128 points -------------------------
-    float yh[KOUT], score;
-    {
-      float x[NIN], xh[KIN];
+    // ---- the network's stress residual: held between evaluations -------
+    // A BF16 network's output moves in quantisation steps while an explicit
+    // step moves the strain by ~1e-6: evaluated every step, those steps act
+    // as a local stiffness several times the elastic one and the explicit
+    // scheme goes unstable (measured: the trajectory parts from FP64 by
+    // 1.5e-2 within 20 steps, against 2e-7 with every point on the plain
+    // law).  So a tile evaluates the network every `period` steps (tiles
+    // staggered) or when one of its points has no residual (a point back
+    // from the plain law), and holds the residual in between; the analytic
+    // part S_p follows the strain every step.
+    float x[NIN];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        x[c] = 0.5f * A2[c];
-        x[6 + c] = etr0[c];
-      }
-      x[12] = (float)tmp;
-      x[13] = (float)xS0;
+    for (int c = 0; c < 6; ++c) {
+      x[c] = 0.5f * A2[c];
+      x[6 + c] = etr0[c];
+    }
+    x[12] = (float)tmp;
+    x[13] = (float)xS0;
+    bool inbox = true;
+#pragma unroll
+    for (int c = 0; c < NIN; ++c) inbox &= (x[c] >= st.lo_x[c] && x[c] <= st.hi_x[c]);
+    float r[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) r[c] = __half2float(s.rcache[c * a.sst + gp]);
+    const int64_t kstep = s.clock ? (int64_t)(s.clock->cutim / s.clock->dtime + 0.5) : 0;
+    const bool due = ((tile + kstep) % s.period) == 0;
+    const bool refresh = __syncthreads_or(due || isnan(r[0]));   // block-uniform
+    float score = inbox ? 0.f : __int_as_float(0x7f800000), xs_inc = 0.f;
+    if (refresh) {
+      float xh[KIN], yh[KOUT];
       score = normalise(st, x, xh);
       if (!mlp_tile(ms, xh, yh)) {
         if (threadIdx.x == 0) atomicExch(s.status, 1);
         break;                                                   // block-uniform
       }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) r[c] = yh[c] * st.sd_y[c] + st.mu_y[c];
+      xs_inc = yh[6] * st.sd_y[6] + st.mu_y[6];
     }
     double tmp2;
     const MatC m = CMP ? compact_mat<float>(a, ec, &tmp2) : a.mat0;
-    float y[NOUT];
-#pragma unroll
-    for (int c = 0; c < NOUT; ++c) y[c] = yh[c] * st.sd_y[c] + st.mu_y[c];
     // ---- stress of the network, loading functions, gates ---------------
     const float Ex = (float)reuss_E(m, xS0);
-    float S[6];
+    float S[6], etr_p[6];
     {
       float E[6], sp[6];
 #pragma unroll
       for (int c = 0; c < 6; ++c) E[c] = 0.5f * A2[c];
-      stress_predictor<float>(m.kK, m.kG, m.alfa, E, etr0, sp);
+      analytic_part<float>(m.kK, m.kG, m.alfa, E, etr0, sp, etr_p);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) S[c] = (y[c] + sp[c]) * Ex;
+      for (int c = 0; c < 6; ++c) S[c] = (r[c] + sp[c]) * Ex;
     }
     double F_AS, F_SA;
     {
@@ -151,15 +179,29 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
       const float t02 = 0.5f * ((C00 * S[5] + C01 * S[4] + C02 * S[2]) + (C02 * S[0] + C12 * S[3] + C22 * S[5]));
       const float p = (t00 + t11 + t22) * (1.f / 3.f);
       const float d0 = t00 - p, d1 = t11 - p, d2 = t22 - p;
+      // the law's deviatoric term 2G (|e| - eL xS0) is signed: dev T points
+      // against the strain deviator once the strain is below the
+      // transformation strain, so |dev T| takes the sign of the projection
+      // of dev T on dev E (whose direction is e's to first order)
+      const float em = (A2[0] + A2[1] + A2[2]) * (1.f / 6.f);
+      const float proj = d0 * (0.5f * A2[0] - em) + d1 * (0.5f * A2[1] - em) + d2 * (0.5f * A2[2] - em) +
+                         (t01 * A2[3] + t12 * A2[4] + t02 * A2[5]);
       const double dn = sqrt((double)(d0 * d0 + d1 * d1 + d2 * d2 + 2.f * (t01 * t01 + t12 * t12 + t02 * t02)));
+      const double trac = proj < 0.f ? -dn : dn;
       const double pr = 3.0 * m.alfa * (double)p;
-      F_AS = dn + pr - m.C_AS * tmp;
-      F_SA = dn + pr - m.C_SA * tmp;
+      F_AS = trac + pr - m.C_AS * tmp;
+      F_SA = trac + pr - m.C_SA * tmp;
     }
-    const bool kf_AS = (F_AS > F_AS0) && (F_AS - m.Rs_AS > 0.0) && (xS0 < 1.0);
-    const bool kf_SA = (F_SA < F_SA0) && (F_SA - m.Rs_SA < 0.0) && (xS0 > 0.0);
+    // A point on or near a transformation surface goes to the law, which
+    // alone decides its activation: the test F > F0 (:351, :368) compares
+    // two loading values one explicit step apart (~0.05 MPa), far below the
+    // network's stress error (~0.5 MPa), so only points at least f_margin
+    // inside the elastic band -- where neither transformation can start
+    // this step -- keep the network's stress.
+    const bool near_AS = (F_AS - m.Rs_AS > -(double)s.f_margin) && (xS0 < 1.0);
+    const bool near_SA = (F_SA - m.Rs_SA < (double)s.f_margin) && (xS0 > 0.0);
     const bool ood = !(score <= s.gate);
-    const bool fallback = ood || kf_AS || kf_SA || !(fabsf(y[6]) <= s.xs_tol);
+    const bool fallback = ood || near_AS || near_SA || !(fabsf(xs_inc) <= s.xs_tol);
     double xS = xS0;
     float etr[6];
     int flag = NR_NONE;
@@ -178,13 +220,12 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
 #pragma unroll
       for (int c = 0; c < 6; ++c) etr[c] = ex * D[c];
     } else {
-      // the transformation strain stays as it is while the return map is
-      // inactive: the network's increment (the turn of D within one step,
-      // a few 1e-3 of eps_tr) is below its BF16 resolution and, added step
-      // after step, would random-walk the state; a point that transforms
-      // again gets eL xS D from the law
+      // the transformation strain of an inactive point: its length eL xS0
+      // turned onto the current direction (analytic_part); the network's
+      // remainder on it (O(E^3) of eps_tr) is below its BF16 resolution and
+      // is not integrated, so its noise cannot random-walk the state
 #pragma unroll
-      for (int c = 0; c < 6; ++c) etr[c] = etr0[c];
+      for (int c = 0; c < 6; ++c) etr[c] = etr_p[c];
     }
     if (valid) {
       a.snew[gp] = (float)xS;
@@ -192,6 +233,11 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
       a.snew[2 * a.sst + gp] = (float)F_SA;
 #pragma unroll
       for (int c = 0; c < 6; ++c) s.etr_new[c * a.sst + gp] = etr[c];
+      // the residual held for the next steps (none after the plain law)
+      if (refresh || fallback)
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+          s.rcache[c * a.sst + gp] = fallback ? __ushort_as_half((unsigned short)0x7fff) : __float2half_rn(r[c]);
     }
     // ---- tau = F S F^T (F = I + H, row-major) and the element forces ----
     float tau[6];

@@ -397,7 +397,8 @@ def ensemble_sizes(nspec=256, seed=0, emin=1000, emax=50000):
     return 10 * k ** 3
 
 
-def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15, subset=None):
+def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15, subset=None,
+             by_size=False):
     """Batched ensemble: nspec independent NiTi specimens (10:1:1 bars, 1 mm
     elements) with element counts drawn log-uniform in [emin, emax] and every
     specimen's E_A, E_M, eps_L and transformation stresses scaled by
@@ -408,9 +409,13 @@ def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15,
     shared smooth load cycle; one dt (0.5 dt_crit of the stiffest specimen).
     `subset` (specimen ids) builds only those specimens -- each specimen's
     random numbers come from its own stream, so a subset is identical to the
-    same specimens of the full ensemble (used to shard across GPUs)."""
+    same specimens of the full ensemble (used to shard across GPUs).
+    by_size concatenates the specimens in increasing size (stable), so each
+    size bucket is one contiguous element range (`size_buckets`)."""
     sizes = ensemble_sizes(nspec, seed, emin, emax)
     ids = list(range(nspec)) if subset is None else [int(v) for v in subset]
+    if by_size:
+        ids = sorted(ids, key=lambda s: (sizes[s], s))
     coords, lnods_l, props_l, em_l, fixno_l, fext_l, spec_of = [], [], [], [], [], [], []
     off = 0
     base = nitinol_props(**NITI)
@@ -451,6 +456,23 @@ def ensemble(nspec=256, nsteps=5000, seed=0, emin=1000, emax=50000, spread=0.15,
                    name=f"ensemble_{nspec}", info=dict(specimens=len(ids), ids=ids,
                                                        elements=int(lnods.shape[0]),
                                                        sizes=[int(v) for v in np.bincount(lmate)]))
+
+
+def size_buckets(prob):
+    """Contiguous element ranges of an ensemble built with by_size=True, one
+    per specimen-size bucket (the element count rounded down to a power of
+    two): [(elements per specimen of the bucket's smallest, end element)]."""
+    sizes = prob.info["sizes"]                               # elements of each local specimen, in order
+    out, end = [], 0
+    cur = None
+    for n in sizes:
+        b = 1 << int(np.floor(np.log2(n)))
+        if cur is not None and b != cur:
+            out.append((cur, end))
+        cur = b
+        end += n
+    out.append((cur, end))
+    return out
 
 
 def cantilever_400x40x40(nsteps=20000, seed=0, ref_equivalent=False, div=1):

@@ -27,7 +27,8 @@ OFF = dict(W1=0, b1=1024, W2=1088, b2=5184, W3=5248, b3=9344, W4=9408, b4=13504,
 class Stats(C.Structure):
     """sma_sur_stats: normalisation and the out-of-envelope gate."""
     _fields_ = [("mu_x", C.c_float * NIN), ("sd_x", C.c_float * NIN), ("mu_y", C.c_float * NOUT),
-                ("sd_y", C.c_float * NOUT), ("linv", C.c_float * (NIN * NIN))]
+                ("sd_y", C.c_float * NOUT), ("linv", C.c_float * (NIN * NIN)),
+                ("lo_x", C.c_float * NIN), ("hi_x", C.c_float * NIN)]
 
 
 def _bind():
@@ -45,7 +46,7 @@ def _bind():
 
 
 def generate(props, e_mart, npath, nstep=512, seed=0, spread=0.10, t_range=(300.0, 320.0),
-             e_range=(-0.05, 0.03), shear=0.004, nseg=4, device=0, inactive_only=False):
+             e_range=(-0.09, 0.06), shear=0.006, nseg=4, device=0, inactive_only=False):
     """Randomised plain-law load paths on the GPU: (x, y) float32 tensors of
     npath * nstep samples (see sma_sur_generate).  inactive_only keeps the
     samples where the law's return map left xS unchanged: the points the
@@ -148,6 +149,9 @@ class Surrogate:
         lv = Linv.astype(np.float32).ravel()
         for i in range(NIN * NIN):
             st.linv[i] = float(lv[i])
+        lo, hi = x.min(0).values.cpu().numpy(), x.max(0).values.cpu().numpy()
+        for i in range(NIN):
+            st.lo_x[i], st.hi_x[i] = float(lo[i]), float(hi[i])
         self._upload_stats()
 
     def _upload_stats(self):

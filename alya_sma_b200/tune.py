@@ -95,3 +95,62 @@ def autotuned(prob, precision="fp32", scheme="cd", device=0, **kw):
     r = tune(prob, precision=precision, scheme=scheme, device=device, **kw)
     return ExplicitSolid(prob, precision=precision, scatter=r["scatter"], block=r["block"],
                          device=device, scheme=scheme, variant=r["variant"])
+
+
+def tune_buckets(prob, precision="fp32", candidates=(32, 64, 128, 256), steps=10, warmup=3, device=0,
+                 displ=None, rounds=1, verbose=False):
+    """Per-size-bucket element blocks for an ensemble built with
+    by_size=True: coordinate descent over the buckets (problem.size_buckets),
+    each bucket's candidates timed with the others at their current pick,
+    the whole step timed by the device phase timers (sma_set_timing) from
+    the same start.  Returns {'plan': [(bucket, end, block)], 'step_ms',
+    'default_step_ms', 'trials'}."""
+    from . import ExplicitSolid
+    from . import problem as P
+    buckets = P.size_buckets(prob)
+    ends = [e for _, e in buckets]
+    s = ExplicitSolid(prob, precision=precision, device=device)
+    if displ is not None:
+        s.set("displ", displ)
+    s.step(warmup)
+    ckpt_state = (s.get("displ"), s.get("veloc"), s.get("accel"), s.state, s.time)
+
+    def timed(blocks):
+        d, v, a, st, tm = ckpt_state
+        s.set("displ", d)
+        s.set("veloc", v)
+        s.set("accel", a)
+        s.state = st
+        s.time = tm
+        s.set_launch_plan(ends, blocks)
+        s.step(1)                                   # graphs and caches of this plan
+        s.set_timing(True)
+        s.step(steps)
+        t = s.timers()
+        s.set_timing(False)
+        return t["step"][0] / steps
+
+    default = [0] * len(ends)
+    default_block = 128 if len(prob.props) > 1 else 32
+    pick = [default_block] * len(ends)
+    base = timed(pick)
+    trials = {}
+    for _ in range(rounds):
+        for r in range(len(ends)):
+            best_b, best_t = pick[r], None
+            for b in candidates:
+                trial = list(pick)
+                trial[r] = b
+                ms = timed(trial)
+                trials[f"{buckets[r][0]}:{b}"] = ms
+                if verbose:
+                    print(f"bucket {buckets[r][0]} block {b}: {ms:.4f} ms/step")
+                if best_t is None or ms < best_t:
+                    best_b, best_t = b, ms
+            pick[r] = best_b
+    final = timed(pick)
+    s.set_launch_plan([], [])
+    s.close()
+    del default
+    return {"plan": [(buckets[r][0], ends[r], pick[r]) for r in range(len(ends))], "step_ms": final,
+            "default_step_ms": base, "default_block": default_block, "trials": trials}

@@ -295,12 +295,14 @@ def build_problem(workload, div, rank=0, world=1, layers=0):
     if workload == "cylinder":
         return P.cylinder_2m(nsteps=10000, div=div, layers=layers or None)
     if workload == "ensemble":
+        # specimens concatenated by size, so each size bucket is one element
+        # range (the autotuner's launch plan gives each its own block)
         nspec = max(2, 256 // div)
         if world > 1:
             from alya_sma_b200 import dist as D
             mine = D.shard_specimens(P.ensemble_sizes(nspec), rank, world)
-            return P.ensemble(nspec=nspec, nsteps=5000, subset=mine)
-        return P.ensemble(nspec=nspec, nsteps=5000)
+            return P.ensemble(nspec=nspec, nsteps=5000, subset=mine, by_size=True)
+        return P.ensemble(nspec=nspec, nsteps=5000, by_size=True)
     return P.cantilever_400x40x40(nsteps=20000, div=div)
 
 
@@ -578,13 +580,18 @@ def main():
 
     from alya_sma_b200 import problem as P
     u0 = P.prestrain(prob, args.prestrain)
-    block, scatter, tuned = args.block, args.scatter, None
-    if args.autotune:
+    block, scatter, tuned, plan = args.block, args.scatter, None, None
+    variant = "auto"
+    if args.autotune and args.workload == "ensemble":
+        # per specimen-size bucket: each bucket's element range its own block
+        from alya_sma_b200 import tune
+        tuned = tune.tune_buckets(prob, precision="fp32" if args.precision == "surrogate" else args.precision,
+                                  displ=u0, device=local)
+        plan = tuned["plan"]
+    elif args.autotune:
         from alya_sma_b200 import tune
         tuned = tune.tune(prob, precision=args.precision, displ=u0, steps=10, warmup=3, device=local)
         block, scatter, variant = tuned["block"], tuned["scatter"], tuned["variant"]
-    else:
-        variant = "auto"
     args.scatter = scatter
     # --precision surrogate: the FP32 form with the learned surrogate in its
     # element loop is the timed form (trained first; the warm-up runs the
@@ -597,6 +604,8 @@ def main():
                                     device=local)
     solid = sma.ExplicitSolid(prob, precision=prec, scatter=scatter, block=block,
                               device=local, variant=variant)
+    if plan:
+        solid.set_launch_plan([e for _, e, _ in plan], [blk for _, _, blk in plan])
     solid.set("displ", u0)
     stream = torch.cuda.ExternalStream(solid.stream)
     solid.step(max(3, args.warmup))
@@ -749,6 +758,8 @@ def main():
                            "gauss_points": ngp_all, "precision": args.precision,
                            "scatter": args.scatter, "block": block or default_block(prob, variant), "variant": variant,
                            "autotuned": bool(tuned), "dtime": prob.dtime,
+                           "launch_plan": ([{"bucket_elements": bk, "end": e, "block": blk} for bk, e, blk in plan]
+                                           if plan else None),
                            "prestrain": args.prestrain,
                            "l2": "working set > L2 (state, nodal arrays and connectivity "
                                  f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",

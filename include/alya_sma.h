@@ -245,11 +245,13 @@ int32_t sma_noalloc_counters(sma_counters* out, void* stream);
  *   x: Green-Lagrange strain E (6), previous transformation strain
  *      eps_tr0 = eL xS0 D0 (6, D0 the unit deviatoric direction of ln U),
  *      temperature, previous martensite fraction xS0
- *   y: (S - S_p) / E(xS0) (6), xS - xS0, eps_tr - eps_tr0 (6), where S is
- *      the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus and S_p
- *      the law's elastic response on a second-order logarithmic strain
- *      ln U ~ E - E^2: T_p = K (tr h - 3 alpha |eps_tr0|) I + 2G (dev h -
- *      eps_tr0), S_p = sym(C^-1 T_p).
+ *   y: (S - S_p) / E(xS0) (6), xS - xS0, eps_tr - eps_tr_p (6), where S is
+ *      the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus, h =
+ *      E - E^2 + 4/3 E^3 (ln U to O(E^4)), eps_tr_p = |eps_tr0| dev h /
+ *      |dev h| (the transformation strain turned onto the current direction,
+ *      as the law keeps it) and S_p the law's elastic response on them:
+ *      T_p = K (tr h - 3 alpha |eps_tr_p|) I + 2G (dev h - eps_tr_p),
+ *      S_p = sym(C^-1 T_p), over E(xS0).
  * Parameters: SMA_SUR_NPARAM FP32 values, padded flat layout W1 [64][16],
  * b1 [64], W2, W3, W4 [64][64], b2, b3, b4 [64], W5 [16][64], b5 [16]
  * (W[o][i]: input i to output o; padding zero).  All pointers d_* are
@@ -266,6 +268,8 @@ typedef struct {
                                                   * (lower, row-major): the         *
                                                   * out-of-envelope score is        *
                                                   * |linv xh| / sqrt(14)            */
+  float lo_x[SMA_SUR_NIN], hi_x[SMA_SUR_NIN];    /* the training inputs' range: an  *
+                                                  * input outside it scores +inf    */
 } sma_sur_stats;
 
 /* Training data: npath randomised load paths of the plain law (FP64,
@@ -305,11 +309,19 @@ int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats
  * of law 160's evaluation in sld_builtin_materials.f90:316-336: the network
  * on the tcgen05 tensor cores for every Gauss point, then the plain law for
  * the points the gates send back -- an out-of-envelope score above `gate`,
- * the law's activation test (sld_stress_model_160.f90:351-374) on the
- * loading functions of the predicted stress (a point about to transform
- * needs the return map), or a predicted martensite increment above
- * `xs_tol` on a point the law leaves inactive (its return-map residual is
- * then not zero).  params: SMA_SUR_NPARAM host FP32 values, stats: host.
+ * loading functions of the predicted stress within `f_margin` (MPa, the
+ * law's deviatoric units) of a transformation start (the law's activation
+ * test, sld_stress_model_160.f90:351-374, compares loading values one step
+ * apart and needs the exact stress there), or a predicted martensite
+ * increment above `xs_tol` on a point the law leaves inactive (its
+ * return-map residual is then not zero).  Accepted points keep xS and turn
+ * the transformation strain onto the current strain direction.  The network's stress residual is evaluated on a
+ * tile of 16 elements every `period` steps (tiles staggered) or when one of
+ * its points has none (back from the plain law) and held in between (FP16
+ * per Gauss point): evaluated every step, the BF16 network's quantisation
+ * steps act as a stiffness the explicit scheme cannot carry; the analytic
+ * part follows the strain every step.  params: SMA_SUR_NPARAM host FP32
+ * values, stats: host.
  * Switching on derives eps_tr from the TIME_N state at the current
  * displacement; enable = 0 returns to the plain law.  Counters: slot 5
  * (SMA_CNT_SUR_FALLBACK) Gauss points sent to the plain law, slot 7
@@ -317,7 +329,7 @@ int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats
 #define SMA_CNT_SUR_FALLBACK 5
 #define SMA_CNT_SUR_OOD      7
 int32_t sma_set_surrogate(sma_ctx* ctx, const float* params, const sma_sur_stats* stats, double gate,
-                          double xs_tol, int32_t enable);
+                          double xs_tol, double f_margin, int32_t period, int32_t enable);
 /* 1 in *status if a wait of the surrogate element loop for the tensor cores
  * ran out since it was switched on (never expected), else 0. */
 int32_t sma_surrogate_status(sma_ctx* ctx, int32_t* status);
@@ -397,6 +409,15 @@ void* sma_stream(sma_ctx* ctx);
 #define SMA_NTIMERS 3
 int32_t sma_set_timing(sma_ctx* ctx, int32_t enable);
 int32_t sma_get_timers(sma_ctx* ctx, double* ms, int64_t* counts);
+
+/* Launch plan of the element loop: nrange element ranges [end[r-1], end[r])
+ * (end[nrange-1] = nelem) each launched with block[r] threads per block (a
+ * multiple of 32 in [32, 256]); nrange = 0 returns to one launch.  For
+ * meshes concatenating specimens of different sizes (the ensemble), sorted
+ * by size bucket, so each bucket gets the block its autotuning picked --
+ * the counterpart of the pack/chunk choice of sld_elmope.f90:66-90
+ * (par_omp_nelem_chunk, VECTOR_SIZE).  Atomic scatter, one-tile kernel. */
+int32_t sma_set_launch_plan(sma_ctx* ctx, int32_t nrange, const int32_t* end, const int32_t* block);
 
 /* kernel launches issued by this context since creation (all kernels) */
 int64_t sma_kernel_launches(sma_ctx* ctx);

@@ -150,3 +150,34 @@ def test_prestrained_start_is_physical(name):
     c = g.counters()
     assert c["neg_det"] == 0 and c["nonfinite"] == 0 and c["ielem_min"] == -1, c
     assert c["nr_active"] > 0                                      # the return map is live
+
+
+def test_launch_plan_by_size_bucket(oracle):
+    """An ensemble concatenated by specimen size has one element range per
+    size bucket; a launch plan gives each range its own block (here a
+    different one per bucket) and the run equals the single launch's and
+    the oracle's.  The bucket autotuner times each bucket's candidates and
+    returns a plan no slower than the default block."""
+    p = P.ensemble(nspec=12, nsteps=400, emin=100, emax=3000, by_size=True)
+    buckets = P.size_buckets(p)
+    assert len(buckets) >= 3 and buckets[-1][1] == p.nelem
+    ends = [e for _, e in buckets]
+    blocks = [(32, 64, 128, 256, 192)[r % 5] for r in range(len(ends))]
+    wit = [3 * int(np.argmax(p.coord[:, 0]))]
+    o = oracle.Problem(p)
+    h_ref = o.run(p.dtime, 120, wit_dof=wit)
+    out = {}
+    for name, plan in (("one", None), ("plan", (ends, blocks))):
+        g = sma.ExplicitSolid(p, precision="fp64")
+        if plan:
+            g.set_launch_plan(*plan)
+        g.set_witness(wit, 120)
+        g.step(120)
+        out[name] = (g.get("displ"), g.witness())
+        g.close()
+    scale = np.abs(out["one"][0]).max()
+    assert np.abs(out["plan"][0] - out["one"][0]).max() <= 1e-10 * scale
+    assert np.abs(out["plan"][1] - h_ref).max() <= 1e-6 * np.abs(h_ref).max()
+    t = tune.tune_buckets(p, precision="fp32", steps=5, warmup=2)
+    assert [e for _, e, _ in t["plan"]] == ends
+    assert t["step_ms"] <= 1.10 * t["default_step_ms"], t
