@@ -2085,10 +2085,26 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(c->stream));
   if (!stage) cudaFree(d_w);
+  // blocks per SM: the occupancy query, or the kernel's own register and
+  // shared-memory needs against the SM's limits where that allows more (the
+  // query has answered 1 for this kernel where 3 blocks fit).  Tiles come
+  // from an atomic counter and no block waits for another, so a block that
+  // is not resident only starts later.
   int per_sm = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, c->compact ? sur::k_element_sur<true>
-                                                                       : sur::k_element_sur<false>,
-                                                   sur::SUR_BLOCK, sur::sur_elem_smem_bytes()));
+  const void* fn = c->compact ? (const void*)sur::k_element_sur<true> : (const void*)sur::k_element_sur<false>;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, sur::SUR_BLOCK, sur::sur_elem_smem_bytes()));
+  {
+    cudaFuncAttributes fa;
+    int regs_sm = 0, smem_sm = 0, smem_res = 0;
+    CU(cudaFuncGetAttributes(&fa, fn));
+    CU(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c->dev));
+    CU(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev));
+    CU(cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, c->dev));
+    const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;         // allocated per warp in 256s
+    const int by_regs = regs_sm / (warp_regs * (sur::SUR_BLOCK / 32));
+    const int by_smem = (int)((size_t)smem_sm / (sur::sur_elem_smem_bytes() + fa.sharedSizeBytes + smem_res));
+    per_sm = std::max(per_sm, std::min(by_regs, by_smem));
+  }
   if (per_sm < 1) return fail(SMA_ERR_ARG, "surrogate element kernel does not fit on an SM");
   c->sur_grid = c->nsm * per_sm;
   c->sur_gate = (float)gate;

@@ -7,8 +7,9 @@
 // 128 Gauss points = one M = 128 tile per block):
 //   1. gather, kinematics (as k_element), E = (C - I)/2;
 //   2. the network on the block's 128 points (tcgen05.mma into TMEM) every
-//      `period` steps per tile (staggered) or when a point has no residual,
-//      the residual held in between (FP16 per Gauss point);
+//      `period` steps per tile (staggered) or when a point has no residual
+//      yet, the residual held in between (FP16 per Gauss point; a point
+//      the plain law handled holds the law's residual);
 //   3. S = E(xS0) (y_S + S_p) (analytic_part: eps_tr turned onto the current
 //      strain direction, as the law keeps it), the rotated-back Kirchhoff stress
 //      T = sym(C S) and from it the law's loading functions
@@ -39,7 +40,7 @@ struct SurElemArgs {
   const SurStats* stats;
   const float* etr_old;       // eps_tr at TIME_N, SoA [6][sst]
   float* etr_new;             // eps_tr at ITER_K
-  __half* rcache;             // the network's stress residual per Gauss point, SoA [6][sst] (NaN: none)
+  __half* rcache;             // the held stress residual per Gauss point, SoA [6][sst] (NaN: none yet)
   const StepTime* clock;      // the step's time (its index picks the tiles that refresh)
   int* tile_ctr;              // next tile (zeroed before the launch)
   int* status;                // set to 1 if a wait for the tensor cores ran out
@@ -118,12 +119,11 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
     // A BF16 network's output moves in quantisation steps while an explicit
     // step moves the strain by ~1e-6: evaluated every step, those steps act
     // as a local stiffness several times the elastic one and the explicit
-    // scheme goes unstable (measured: the trajectory parts from FP64 by
-    // 1.5e-2 within 20 steps, against 2e-7 with every point on the plain
-    // law).  So a tile evaluates the network every `period` steps (tiles
-    // staggered) or when one of its points has no residual (a point back
-    // from the plain law), and holds the residual in between; the analytic
-    // part S_p follows the strain every step.
+    // scheme drifts.  So a tile evaluates the network every `period` steps
+    // (tiles staggered) or when one of its points has no residual yet (NaN,
+    // the first step), and holds the residual in between; a point the plain
+    // law handled holds the law's residual; the analytic part S_p follows
+    // the strain every step.
     float x[NIN];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
@@ -219,6 +219,16 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
       const float ex = (float)(m.eL * xS);
 #pragma unroll
       for (int c = 0; c < 6; ++c) etr[c] = ex * D[c];
+      // the law's own residual against the state the next step starts from
+      // (xS, eps_tr): held like the network's, so a tile with points back
+      // from the law needs no extra evaluation of the network
+      float E[6], sp[6], ep[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) E[c] = 0.5f * A2[c];
+      analytic_part<float>(m.kK, m.kG, m.alfa, E, etr, sp, ep);
+      const float rE = (float)(1.0 / reuss_E(m, xS));
+#pragma unroll
+      for (int c = 0; c < 6; ++c) r[c] = S[c] * rE - sp[c];
     } else {
       // the transformation strain of an inactive point: its length eL xS0
       // turned onto the current direction (analytic_part); the network's
@@ -233,11 +243,11 @@ __global__ void __launch_bounds__(SUR_BLOCK, 3) k_element_sur(ElemArgs<float> a,
       a.snew[2 * a.sst + gp] = (float)F_SA;
 #pragma unroll
       for (int c = 0; c < 6; ++c) s.etr_new[c * a.sst + gp] = etr[c];
-      // the residual held for the next steps (none after the plain law)
+      // the residual held for the next steps: the network's after an
+      // evaluation, the law's after a fallback
       if (refresh || fallback)
 #pragma unroll
-        for (int c = 0; c < 6; ++c)
-          s.rcache[c * a.sst + gp] = fallback ? __ushort_as_half((unsigned short)0x7fff) : __float2half_rn(r[c]);
+        for (int c = 0; c < 6; ++c) s.rcache[c * a.sst + gp] = __float2half_rn(r[c]);
     }
     // ---- tau = F S F^T (F = I + H, row-major) and the element forces ----
     float tau[6];
