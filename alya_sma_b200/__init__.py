@@ -273,8 +273,8 @@ class ExplicitSolid:
         if reset:
             _check(lib().sma_reset_counters(self._ctx))
         out = {name: int(c.c[i]) for i, name in enumerate(COUNTERS)}
-        out["sur_fallback"] = int(c.c[5])                     # surrogate points sent to the plain law
-        out["sur_ood"] = int(c.c[7])                          # of those, out of the envelope
+        out["sur_fallback"] = int(c.c[5])                     # surrogate points the plain law handled
+        out["sur_ood"] = int(c.c[7])                          # network evaluations its gates refused
         out["gpdet_min"] = float(c.gpdet_min)                 # smallest det F <= 0, 0.0 if none
         out["ielem_min"] = int(c.ielem_min)                   # its element, -1 if none
         return out

@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libalya_sma_b200.so")
 SOURCES = ["sma_capi.cu", "sma_surrogate.cu"]
-HEADERS = ["sma_law.cuh", "sma_kernels.cuh", "sma_surrogate.cuh"]
+HEADERS = ["sma_law.cuh", "sma_kernels.cuh", "sma_surrogate.cuh", "sma_surrogate_elem.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]

@@ -252,12 +252,13 @@ struct sma_ctx {
   bool sur = false;
   unsigned char* d_sur_img = nullptr;
   sur::SurStats* d_sur_stats = nullptr;
-  float* d_etr[2] = {nullptr, nullptr};    // [6][sst] per state buffer
-  __half* d_rcache = nullptr;              // the network's held residual, [6][sst] FP16
+  __half* d_rcache = nullptr;              // held stress residual, [6][sst] FP16 (NaN: none)
+  float* d_xstage = nullptr;               // network inputs of the due tiles, [slot][14][128]
+  int64_t xstage_slots = 0;
   int sur_period = 64;
-  int* d_sur_ctr = nullptr;                // [0] tile counter, [1] status
+  int* d_sur_ctr = nullptr;                // [1] status of the tensor-core waits
   float sur_gate = 3.0f, sur_xs_tol = 1e-3f, sur_margin = 10.0f;
-  int sur_grid = 0;
+  int sur_grid = 0;                        // persistent grid of the network kernel
   void* d_state[2] = {nullptr, nullptr};   // T [3][sst]
   int cur = 0;                             // state buffer holding TIME_N
   int last_in = -1;                        // state buffer the last element loop read (-1: none)
@@ -447,30 +448,52 @@ int32_t init_element_launch_t(sma_ctx* c) {
   return SMA_OK;
 }
 
-// the surrogate element kernel on elements [beg, end): persistent blocks,
-// tiles handed out by a counter cleared first (a memset node in graphs)
+sur::SurElemArgs sur_args(const sma_ctx* c) {
+  sur::SurElemArgs s;
+  s.stats = c->d_sur_stats;
+  s.rcache = c->d_rcache;
+  s.xstage = c->d_xstage;
+  s.clock = c->d_ts;
+  s.f_margin = c->sur_margin;
+  s.period = c->sur_period;
+  return s;
+}
+
+// the surrogate element kernel on elements [beg, end): one block per tile of
+// 16 elements, tiles numbered over the whole mesh (a range that starts or
+// ends inside a tile leaves the tile's other lanes idle)
 int32_t launch_sur_range(sma_ctx* c, int beg, int end, bool advance, bool stepping) {
   if (end <= beg) return SMA_OK;
   ElemArgs<float> a = elem_args<float>(c, beg, end, advance, stepping);
-  sur::SurElemArgs s;
-  s.img = c->d_sur_img;
-  s.stats = c->d_sur_stats;
-  s.etr_old = c->d_etr[c->cur];
-  s.etr_new = c->d_etr[c->cur ^ 1];
-  s.tile_ctr = c->d_sur_ctr;
-  s.status = c->d_sur_ctr + 1;
-  s.gate = c->sur_gate;
-  s.xs_tol = c->sur_xs_tol;
-  s.f_margin = c->sur_margin;
-  s.rcache = c->d_rcache;
-  s.clock = c->d_ts;
-  s.period = c->sur_period;
-  CU(cudaMemsetAsync(c->d_sur_ctr, 0, sizeof(int), c->stream));
-  const int64_t ntiles = ceil_div(end - beg, sur::SUR_EPB);
-  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, c->sur_grid);
-  const size_t smem = sur::sur_elem_smem_bytes();
-  if (c->compact) sur::k_element_sur<true><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
-  else sur::k_element_sur<false><<<grid, sur::SUR_BLOCK, smem, c->stream>>>(a, s);
+  const sur::SurElemArgs s = sur_args(c);
+  const unsigned grid = (unsigned)((end - 1) / sur::SUR_EPB - beg / sur::SUR_EPB + 1);
+  if (c->compact) sur::k_element_sur<true><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, s);
+  else sur::k_element_sur<false><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, s);
+  c->launches++;
+  CU(cudaGetLastError());
+  return SMA_OK;
+}
+
+// the network on the tiles staged in residue class cls (< 0: the running
+// step's due tiles, after the step's element ranges and before its nodal
+// update, which moves the step time)
+int32_t launch_sur_refresh(sma_ctx* c, int cls) {
+  sur::RefreshArgs r;
+  r.img = c->d_sur_img;
+  r.stats = c->d_sur_stats;
+  r.xstage = c->d_xstage;
+  r.rcache = c->d_rcache;
+  r.clock = c->d_ts;
+  r.cnt = cls < 0 ? c->d_cnt : nullptr;                         // the switch-on passes count nothing
+  r.status = c->d_sur_ctr + 1;
+  r.sst = c->sst;
+  r.nelem = c->nelem;
+  r.cls = cls;
+  r.period = c->sur_period;
+  r.gate = c->sur_gate;
+  r.xs_tol = c->sur_xs_tol;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(c->xstage_slots, c->sur_grid));
+  sur::k_sur_refresh<<<grid, sur::SUR_BLOCK, sur::mlp_smem_bytes(), c->stream>>>(r);
   c->launches++;
   CU(cudaGetLastError());
   return SMA_OK;
@@ -506,7 +529,8 @@ int32_t launch_elements_t(sma_ctx* c, bool advance) {
   if constexpr (sizeof(T) == 4) {
     if (c->sur) {
       c->last_in = c->cur;
-      return launch_sur_range(c, 0, c->nelem, advance, advance);
+      const int32_t rc = launch_sur_range(c, 0, c->nelem, advance, advance);
+      return (rc || !advance) ? rc : launch_sur_refresh(c, -1);
     }
   }
   if (!c->plan_end.empty()) {
@@ -817,7 +841,8 @@ int64_t kernels_per_step(const sma_ctx* c) {
     for (size_t r = 0; r < c->plan_end.size(); ++r)
       elem += c->plan_end[r] > (r ? c->plan_end[r - 1] : 0);
   }
-  return elem + 1 + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0) + (c->energy && c->damp ? 1 : 0);
+  return elem + 1 + (c->sur ? 1 : 0) + (c->nwit > 0 ? 1 : 0) + (c->energy ? 1 : 0) +
+         (c->energy && c->damp ? 1 : 0);
 }
 
 template <typename T>
@@ -845,7 +870,7 @@ int32_t sma_ctx_destroy(sma_ctx* c) {
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->l2_window) cudaCtxResetPersistingL2Cache();   // release the lines this context pinned
   void* bufs[] = {c->d_lnods, c->d_perm, c->d_lmate, c->d_nodal, c->d_matx, c->d_sur_img, c->d_sur_stats,
-                  c->d_etr[0], c->d_etr[1], c->d_sur_ctr, c->d_rcache,
+                  c->d_xstage, c->d_sur_ctr, c->d_rcache,
                   c->d_invm, c->d_fext, c->d_tempe, c->d_flags, c->d_bcfun, c->d_mats,
                   c->d_state[0], c->d_state[1], c->d_cnt, c->d_ts, c->d_ft, c->d_stage,
                   c->d_stage2, c->d_wdof, c->d_whist, c->d_wrow, c->d_uprev, c->d_fintp,
@@ -1232,6 +1257,7 @@ int32_t sma_step_elements_range(sma_ctx* c, int32_t beg, int32_t end, int32_t fi
     CU(cudaGetLastError());
   }
   if (rc) return rc;
+  if (last && c->prec == SMA_PREC_FP32 && c->sur && (rc = launch_sur_refresh(c, -1))) return rc;
   if (last) {
     c->cur ^= 1;
     if ((rc = launch_witness(c))) return rc;
@@ -2055,14 +2081,44 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
     if ((rc = dalloc(&c->d_sur_img, sur::IMG_BYTES))) return rc;
     if ((rc = dalloc(&c->d_sur_stats, sizeof(sur::SurStats)))) return rc;
     if ((rc = dalloc(&c->d_sur_ctr, 2 * sizeof(int)))) return rc;
-    for (int b = 0; b < 2; ++b)
-      if ((rc = dalloc(&c->d_etr[b], 6 * (size_t)c->sst * sizeof(float)))) return rc;
     if ((rc = dalloc(&c->d_rcache, 6 * (size_t)c->sst * sizeof(__half)))) return rc;
-    CU(cudaFuncSetAttribute(sur::k_element_sur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sur::sur_elem_smem_bytes()));
-    CU(cudaFuncSetAttribute(sur::k_element_sur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sur::sur_elem_smem_bytes()));
+    CU(cudaFuncSetAttribute(sur::k_sur_refresh, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sur::mlp_smem_bytes()));
   }
+  // staging rows: the due tiles of one step, ceil(tiles / period)
+  const int64_t ntiles = ceil_div(c->nelem, sur::SUR_EPB);
+  const int64_t slots = ceil_div(ntiles, period);
+  if (slots > c->xstage_slots) {
+    if (c->d_xstage) cudaFree(c->d_xstage);
+    c->d_xstage = nullptr;
+    c->xstage_slots = 0;
+    if ((rc = dalloc(&c->d_xstage, (size_t)slots * sur::NIN * sur::SUR_BLOCK * sizeof(float)))) return rc;
+    c->xstage_slots = slots;
+  }
+  // the network kernel's persistent grid: blocks per SM by the occupancy
+  // query, or by its register and shared-memory needs against the SM's
+  // limits where that allows more (no block waits for another)
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur::k_sur_refresh, sur::SUR_BLOCK,
+                                                   sur::mlp_smem_bytes()));
+  {
+    cudaFuncAttributes fa;
+    int regs_sm = 0, smem_sm = 0, smem_res = 0;
+    CU(cudaFuncGetAttributes(&fa, sur::k_sur_refresh));
+    CU(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c->dev));
+    CU(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev));
+    CU(cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, c->dev));
+    const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;         // allocated per warp in 256s
+    const int by_regs = regs_sm / (warp_regs * (sur::SUR_BLOCK / 32));
+    const int by_smem = (int)((size_t)smem_sm / (sur::mlp_smem_bytes() + fa.sharedSizeBytes + smem_res));
+    per_sm = std::max(per_sm, std::min(by_regs, by_smem));
+  }
+  if (per_sm < 1) return fail(SMA_ERR_ARG, "surrogate network kernel does not fit on an SM");
+  c->sur_grid = c->nsm * per_sm;
+  c->sur_gate = (float)gate;
+  c->sur_xs_tol = (float)xs_tol;
+  c->sur_margin = (float)f_margin;
+  c->sur_period = period;
   // parameters through the staging buffer (>= 14,608 floats for any mesh of
   // at least 1,218 nodes; else a temporary), packed into the weight image
   float* d_w = nullptr;
@@ -2075,42 +2131,22 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   CU(cudaMemcpyAsync(c->d_sur_stats, stats, sizeof(sur::SurStats), cudaMemcpyHostToDevice, c->stream));
   CU(cudaMemsetAsync(c->d_sur_ctr, 0, 2 * sizeof(int), c->stream));
   CU(cudaMemsetAsync(c->d_rcache, 0xff, 6 * (size_t)c->sst * sizeof(__half), c->stream));   // NaN: none held
-  // eps_tr of the TIME_N state at the current displacement
+  // the first residual of every point: the network on the TIME_N state at
+  // the current displacement, one residue class of tiles at a time
   {
     ElemArgs<float> a = elem_args<float>(c, 0, c->nelem, false, false);
-    const unsigned grid = (unsigned)ceil_div(c->nelem, 16);
-    if (c->compact) sur::k_sur_etr_init<true><<<grid, 128, 0, c->stream>>>(a, c->d_etr[c->cur]);
-    else sur::k_sur_etr_init<false><<<grid, 128, 0, c->stream>>>(a, c->d_etr[c->cur]);
+    const sur::SurElemArgs sa = sur_args(c);
+    for (int cls = 0; cls < period && cls < ntiles; ++cls) {
+      const unsigned grid = (unsigned)ceil_div(ntiles - cls, period);
+      if (c->compact) sur::k_sur_stage<true><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
+      else sur::k_sur_stage<false><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
+      CU(cudaGetLastError());
+      if ((rc = launch_sur_refresh(c, cls))) return rc;
+    }
   }
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(c->stream));
   if (!stage) cudaFree(d_w);
-  // blocks per SM: the occupancy query, or the kernel's own register and
-  // shared-memory needs against the SM's limits where that allows more (the
-  // query has answered 1 for this kernel where 3 blocks fit).  Tiles come
-  // from an atomic counter and no block waits for another, so a block that
-  // is not resident only starts later.
-  int per_sm = 0;
-  const void* fn = c->compact ? (const void*)sur::k_element_sur<true> : (const void*)sur::k_element_sur<false>;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, sur::SUR_BLOCK, sur::sur_elem_smem_bytes()));
-  {
-    cudaFuncAttributes fa;
-    int regs_sm = 0, smem_sm = 0, smem_res = 0;
-    CU(cudaFuncGetAttributes(&fa, fn));
-    CU(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c->dev));
-    CU(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev));
-    CU(cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, c->dev));
-    const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;         // allocated per warp in 256s
-    const int by_regs = regs_sm / (warp_regs * (sur::SUR_BLOCK / 32));
-    const int by_smem = (int)((size_t)smem_sm / (sur::sur_elem_smem_bytes() + fa.sharedSizeBytes + smem_res));
-    per_sm = std::max(per_sm, std::min(by_regs, by_smem));
-  }
-  if (per_sm < 1) return fail(SMA_ERR_ARG, "surrogate element kernel does not fit on an SM");
-  c->sur_grid = c->nsm * per_sm;
-  c->sur_gate = (float)gate;
-  c->sur_xs_tol = (float)xs_tol;
-  c->sur_margin = (float)f_margin;
-  c->sur_period = period;
   destroy_graphs(c);
   c->sur = true;
   return SMA_OK;

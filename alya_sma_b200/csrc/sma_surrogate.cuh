@@ -10,15 +10,15 @@
 // Network: 14 inputs -> 64 -> 64 -> 64 -> 64 -> 13 outputs, SiLU after the
 // hidden layers.  Per Gauss point, in the material frame (tensors as
 // xx, yy, zz, xy, yz, xz):
-//   inputs   E (Green-Lagrange strain, 6), eps_tr of the previous step (the
-//            transformation strain eL xS D, D the unit deviatoric direction
-//            of ln U, 6), temperature, xS of the previous step
+//   inputs   E (Green-Lagrange strain, 6), eps_tr_p = eL xS0 dev h / |dev h|
+//            (the previous step's transformation strain on the current
+//            deviatoric direction, h ~ ln U; 6), temperature, xS0 (the
+//            previous step's martensite fraction)
 //   outputs  (S - S_p) / E(xS0) (6): the second Piola-Kirchhoff stress less
 //            its analytic part S_p (analytic_part: the law's elastic
-//            response on a third-order logarithmic strain, the
-//            transformation strain turned onto the current direction), over
-//            the Reuss modulus, so the network carries only the remainder;
-//            xS - xS0; eps_tr - eps_tr_p (6), eps_tr_p the turned eps_tr0
+//            response on a third-order logarithmic strain with eps_tr_p),
+//            over the Reuss modulus, so the network carries only the
+//            remainder; xS - xS0; eps_tr - eps_tr_p (6)
 // Inputs and outputs are normalised per feature by the training set's mean
 // and standard deviation (SurStats).  Weights are BF16 with FP32
 // accumulation on the tensor cores; biases and the epilogue are FP32.
@@ -98,15 +98,15 @@ __device__ __forceinline__ void lin_elastic(double kK, double kG, const T* e, T*
 
 // The analytic part of the response.  h = E - E^2 + 4/3 E^3 is ln U to
 // O(E^4) (E the Green-Lagrange strain, C = I + 2E).  The law's transformation
-// strain always lies along the current deviatoric direction (eL xS D,
-// sld_stress_model_160.f90:487-491), so the previous step's eps_tr0 is turned
-// onto dev h: eps_tr = |eps_tr0| dev h / |dev h|.  Then
-// T_p = kK (tr h - 3 alpha |eps_tr|) I + 2 kG (dev h - eps_tr) and
+// strain always lies along the current deviatoric direction with length
+// eL xS (eps_tr = eL xS D, sld_stress_model_160.f90:487-491), so it is no
+// state of its own: eps_tr = ntr dev h / |dev h| with ntr = eL xS0.  Then
+// T_p = kK (tr h - 3 alpha ntr) I + 2 kG (dev h - eps_tr) and
 // S_p = sym(C^-1 T_p) -- the law's elastic response over E(xS0), so the
 // network carries only the O(E^4) remainder.
 template <typename T>
-__device__ __forceinline__ void analytic_part(double kK, double kG, double alfa, const T* E, const T* etr0,
-                                              T* Sp, T* etr) {
+__device__ __forceinline__ void analytic_part(double kK, double kG, double alfa, const T* E, T ntr, T* Sp,
+                                              T* etr) {
   // E^2 and E^3 (symmetric products, xx yy zz xy yz xz)
   T q[6];
   q[0] = E[0] * E[0] + E[3] * E[3] + E[5] * E[5];
@@ -129,16 +129,9 @@ __device__ __forceinline__ void analytic_part(double kK, double kG, double alfa,
   const T tr = h[0] + h[1] + h[2], t3 = tr * (T(1) / T(3));
   const T dh[6] = {h[0] - t3, h[1] - t3, h[2] - t3, h[3], h[4], h[5]};
   const T ndh = sqrt(dh[0] * dh[0] + dh[1] * dh[1] + dh[2] * dh[2] + T(2) * (dh[3] * dh[3] + dh[4] * dh[4] + dh[5] * dh[5]));
-  const T ntr = sqrt(etr0[0] * etr0[0] + etr0[1] * etr0[1] + etr0[2] * etr0[2] +
-                     T(2) * (etr0[3] * etr0[3] + etr0[4] * etr0[4] + etr0[5] * etr0[5]));
-  if (ndh > T(1e-12)) {
-    const T sc = ntr / ndh;
+  const T sc = ndh > T(1e-12) ? ntr / ndh : T(0);              // no direction: no deviatoric strain
 #pragma unroll
-    for (int k = 0; k < 6; ++k) etr[k] = sc * dh[k];
-  } else {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) etr[k] = etr0[k];
-  }
+  for (int k = 0; k < 6; ++k) etr[k] = sc * dh[k];
   const T pv = (T)kK * (tr - T(3) * (T)alfa * ntr), g2 = T(2) * (T)kG;
   const T Tp[6] = {pv + g2 * (dh[0] - etr[0]), pv + g2 * (dh[1] - etr[1]), pv + g2 * (dh[2] - etr[2]),
                    g2 * (dh[3] - etr[3]), g2 * (dh[4] - etr[4]), g2 * (dh[5] - etr[5])};
@@ -164,6 +157,11 @@ __device__ __forceinline__ void analytic_part(double kK, double kG, double alfa,
 // Reuss modulus at the start-of-step fraction (the law's extension rule)
 __device__ __forceinline__ double reuss_E(const MatC& m, double xS0) {
   return 1.0 / ((1.0 - xS0) * m.iEA + xS0 * m.iEM);
+}
+// its inverse in FP32 (the stress scale of the FP32 element loop)
+__device__ __forceinline__ float reuss_iE_f(const MatC& m, double xS0) {
+  const float x = (float)xS0;
+  return (1.f - x) * (float)m.iEA + x * (float)m.iEM;
 }
 
 // ---------------------------------------------------------------------------
@@ -257,7 +255,7 @@ static __global__ void k_sur_generate(GenArgs g) {
   double H0[6] = {0, 0, 0, 0, 0, 0}, H1[6];
   target(H1);
   const int per = (g.nstep + g.nseg - 1) / g.nseg;
-  double xS = 0.0, F_AS = 0.0, F_SA = 0.0, etr[6] = {0, 0, 0, 0, 0, 0};
+  double xS = 0.0, F_AS = 0.0, F_SA = 0.0;
   double Hp[6] = {0, 0, 0, 0, 0, 0};                             // the path's last stretch
   for (int s = 0; s < g.nstep; ++s) {
     const int k = s % per;
@@ -289,10 +287,7 @@ static __global__ void k_sur_generate(GenArgs g) {
     if (pass == 1) {                                             // the path's step: state only
       double Tm[6], D[6];
       law160_from_A<double>(m, A, tmp, xS, F_AS, F_SA, Tm, D);
-      for (int c = 0; c < 6; ++c) {
-        etr[c] = m.eL * xS * D[c];
-        Hp[c] = Hn[c];
-      }
+      for (int c = 0; c < 6; ++c) Hp[c] = Hn[c];
       continue;
     }
     const double xS0 = xS;
@@ -310,10 +305,10 @@ static __global__ void k_sur_generate(GenArgs g) {
     float* yo = g.y + (path * g.nstep + s) * NOUT;
     double E[6], sl[6], er[6];
     for (int c = 0; c < 6; ++c) E[c] = 0.5 * A[c];
-    analytic_part<double>(m.kK, m.kG, m.alfa, E, etr, sl, er);
+    analytic_part<double>(m.kK, m.kG, m.alfa, E, m.eL * xS0, sl, er);
     for (int c = 0; c < 6; ++c) {
       xo[c] = (float)E[c];
-      xo[6 + c] = (float)etr[c];
+      xo[6 + c] = (float)er[c];
       yo[c] = (float)(S[c] / Ex - sl[c]);
     }
     xo[12] = (float)tmp;
@@ -385,7 +380,7 @@ struct TrainArgs {
 template <int KB, int NT>
 __device__ __forceinline__ void fwd_layer(float (*C)[NT][4], const uint32_t (*A)[KB][4], const __nv_bfloat16* W,
                                           int pitch, const float* bias, int lane) {
-  const int g = lane >> 2, t = lane & 3;
+  const int t = lane & 3;
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -954,8 +949,8 @@ __device__ __forceinline__ float normalise(const SurStats& st, const float* x, f
 // Persistent blocks of 128 threads; status[0] set to 1 if a wait ran out.
 static __global__ void __launch_bounds__(128) k_sur_forward(const unsigned char* img, const SurStats* stats, int64_t n,
                                                      const float* x, float* y, float* score, int* status) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023));
+  extern __shared__ __align__(1024) unsigned char mlp_smem_raw[];
+  MlpSmem& s = *reinterpret_cast<MlpSmem*>(mlp_smem_raw + ((1024 - (smem_u32(mlp_smem_raw) & 1023)) & 1023));
   mlp_setup(s, img);
   const SurStats& st = *stats;
   const int64_t ntiles = (n + 127) / 128;

@@ -247,6 +247,24 @@ class Surrogate:
         return w.cpu().numpy()
 
 
+class ZeroResidual:
+    """The surrogate's element loop with the network's output held at zero:
+    the analytic part alone (the law's elastic response on a third-order
+    logarithmic strain), with the same gates and plain-law fallback -- the
+    method without the learned part, for comparisons.  It keeps a trained
+    network's statistics (input box and envelope), so the same points go to
+    the plain law; zero weights and a zero output mean make every stress
+    residual and predicted martensite increment zero."""
+
+    def __init__(self, net):
+        self.stats_host = Stats.from_buffer_copy(bytes(net.stats_host))
+        for i in range(7):
+            self.stats_host.mu_y[i] = 0.0
+
+    def params(self):
+        return np.zeros(NPARAM, np.float32)
+
+
 def training_setup(prob):
     """The generator's material, spread and temperature range for a problem:
     the mean of its per-element materials (sampled symmetrically around a

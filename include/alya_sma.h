@@ -242,15 +242,14 @@ int32_t sma_noalloc_counters(sma_counters* out, void* stream);
  * Network 14 -> 64 -> 64 -> 64 -> 64 -> 13 (SiLU), BF16 weights with FP32
  * accumulation on the tensor cores, per Gauss point in the material frame
  * (tensors xx, yy, zz, xy, yz, xz):
- *   x: Green-Lagrange strain E (6), previous transformation strain
- *      eps_tr0 = eL xS0 D0 (6, D0 the unit deviatoric direction of ln U),
- *      temperature, previous martensite fraction xS0
+ *   x: Green-Lagrange strain E (6), eps_tr_p = eL xS0 dev h / |dev h| (the
+ *      previous step's transformation strain on the current deviatoric
+ *      direction; h = E - E^2 + 4/3 E^3, ln U to O(E^4); 6), temperature,
+ *      previous martensite fraction xS0
  *   y: (S - S_p) / E(xS0) (6), xS - xS0, eps_tr - eps_tr_p (6), where S is
- *      the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus, h =
- *      E - E^2 + 4/3 E^3 (ln U to O(E^4)), eps_tr_p = |eps_tr0| dev h /
- *      |dev h| (the transformation strain turned onto the current direction,
- *      as the law keeps it) and S_p the law's elastic response on them:
- *      T_p = K (tr h - 3 alpha |eps_tr_p|) I + 2G (dev h - eps_tr_p),
+ *      the second Piola-Kirchhoff stress, E(xS0) the Reuss modulus and S_p
+ *      the law's elastic response on h and eps_tr_p:
+ *      T_p = K (tr h - 3 alpha eL xS0) I + 2G (dev h - eps_tr_p),
  *      S_p = sym(C^-1 T_p), over E(xS0).
  * Parameters: SMA_SUR_NPARAM FP32 values, padded flat layout W1 [64][16],
  * b1 [64], W2, W3, W4 [64][64], b2, b3, b4 [64], W5 [16][64], b5 [16]
@@ -306,32 +305,36 @@ int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats
                         float* d_y, float* d_score, int32_t* d_status, void* stream);
 /* The surrogate in a context's element loop (FP32 precision form, atomic
  * scatter, undamped; per-element materials as compact records), in place
- * of law 160's evaluation in sld_builtin_materials.f90:316-336: the network
- * on the tcgen05 tensor cores for every Gauss point, then the plain law for
- * the points the gates send back -- an out-of-envelope score above `gate`,
- * loading functions of the predicted stress within `f_margin` (MPa, the
- * law's deviatoric units) of a transformation start (the law's activation
- * test, sld_stress_model_160.f90:351-374, compares loading values one step
- * apart and needs the exact stress there), or a predicted martensite
- * increment above `xs_tol` on a point the law leaves inactive (its
- * return-map residual is then not zero).  Accepted points keep xS and turn
- * the transformation strain onto the current strain direction.  The network's stress residual is evaluated on a
- * tile of 16 elements every `period` steps (tiles staggered) or when one of
- * its points has none (back from the plain law) and held in between (FP16
- * per Gauss point): evaluated every step, the BF16 network's quantisation
- * steps act as a stiffness the explicit scheme cannot carry; the analytic
- * part follows the strain every step.  params: SMA_SUR_NPARAM host FP32
- * values, stats: host.
- * Switching on derives eps_tr from the TIME_N state at the current
- * displacement; enable = 0 returns to the plain law.  Counters: slot 5
- * (SMA_CNT_SUR_FALLBACK) Gauss points sent to the plain law, slot 7
- * (SMA_CNT_SUR_OOD) of those, out of the envelope. */
+ * of law 160's evaluation in sld_builtin_materials.f90:316-336.  Per Gauss
+ * point the stress is E(xS0) (r + S_p): S_p the analytic part above,
+ * following the strain every step, r a residual held per point (FP16).
+ * The network (tcgen05 tensor cores) evaluates r on each tile of 16
+ * elements every `period` steps (tiles staggered: one tile in `period` per
+ * step) from the inputs the element loop stages for it; held between
+ * evaluations, because a BF16 network evaluated every step moves in
+ * quantisation steps the explicit scheme cannot carry.  The plain law
+ * handles, and then holds its own residual for, a point with no residual
+ * (the network's evaluation was refused: out-of-envelope score above
+ * `gate`, or a predicted martensite increment above `xs_tol`, i.e. a point
+ * the law would transform), an input outside the training inputs' range,
+ * or loading functions of the surrogate's stress within `f_margin` (MPa,
+ * the law's deviatoric units) of a transformation start (the law's
+ * activation test, sld_stress_model_160.f90:351-374, compares loading
+ * values one step apart and needs the exact stress there).  Accepted points
+ * keep xS; the transformation strain is eL xS on the current strain
+ * direction, as the law keeps it.  params: SMA_SUR_NPARAM host FP32
+ * values, stats: host.  Switching on evaluates the network once on every
+ * point at the TIME_N state and the current displacement; enable = 0
+ * returns to the plain law.  A step with the surrogate launches the element
+ * kernel and the network kernel.  Counters: slot 5 (SMA_CNT_SUR_FALLBACK)
+ * Gauss points the plain law handled, slot 7 (SMA_CNT_SUR_OOD) network
+ * evaluations its gates refused. */
 #define SMA_CNT_SUR_FALLBACK 5
 #define SMA_CNT_SUR_OOD      7
 int32_t sma_set_surrogate(sma_ctx* ctx, const float* params, const sma_sur_stats* stats, double gate,
                           double xs_tol, double f_margin, int32_t period, int32_t enable);
-/* 1 in *status if a wait of the surrogate element loop for the tensor cores
- * ran out since it was switched on (never expected), else 0. */
+/* 1 in *status if a wait of the surrogate's network kernel for the tensor
+ * cores ran out since it was switched on (never expected), else 0. */
 int32_t sma_surrogate_status(sma_ctx* ctx, int32_t* status);
 
 /* host <-> context data */
