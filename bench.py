@@ -277,13 +277,15 @@ def per_element_values(prob):
 
 def algorithmic_bytes(prob, precision):
     """Minimum HBM traffic of one element-kernel launch: connectivity, state
-    read + write (with the surrogate also the transformation strain, 6
-    words per Gauss point), the per-element material values and temperature
-    (in the precision's word), one read of coordinates and displacements and
-    one read-modify-write of the residual per node."""
+    read + write (3 words per Gauss point), the per-element material values
+    and temperature (in the precision's word), one read of coordinates and
+    displacements and one read-modify-write of the residual per node; with
+    the surrogate also the held stress residual read (6 FP16 per Gauss
+    point; its writes by the plain law's points and the network's inputs
+    staged for 1/64 of the tiles are not counted)."""
     s = 8 if precision == "fp64" else 4
-    nstate = 9 if precision == "surrogate" else 3
-    return prob.nelem * (32 + 2 * 8 * nstate * s + per_element_values(prob) * s) + prob.npoin * (24 + 24 + 48)
+    held = 8 * 6 * 2 if precision == "surrogate" else 0
+    return prob.nelem * (32 + 2 * 8 * 3 * s + held + per_element_values(prob) * s) + prob.npoin * (24 + 24 + 48)
 
 
 def build_problem(workload, div, rank=0, world=1, layers=0):
