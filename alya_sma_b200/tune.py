@@ -103,7 +103,11 @@ def tune_buckets(prob, precision="fp32", candidates=(32, 64, 128, 256), steps=10
     by_size=True: coordinate descent over the buckets (problem.size_buckets),
     each bucket's candidates timed with the others at their current pick,
     the whole step timed by the device phase timers (sma_set_timing) from
-    the same start.  Returns {'plan': [(bucket, end, block)], 'step_ms',
+    the same start.  Adjacent buckets with the same pick are merged into one
+    range (each range is one launch per step), and the plan is kept only if
+    it beats the library's single launch at its default block, both timed
+    again from the same start (best of three).  Returns {'plan': [(bucket,
+    end, block)] or [] (the single default launch), 'step_ms',
     'default_step_ms', 'trials'}."""
     from . import ExplicitSolid
     from . import problem as P
@@ -115,14 +119,14 @@ def tune_buckets(prob, precision="fp32", candidates=(32, 64, 128, 256), steps=10
     s.step(warmup)
     ckpt_state = (s.get("displ"), s.get("veloc"), s.get("accel"), s.state, s.time)
 
-    def timed(blocks):
+    def timed(plan_ends, blocks):
         d, v, a, st, tm = ckpt_state
         s.set("displ", d)
         s.set("veloc", v)
         s.set("accel", a)
         s.state = st
         s.time = tm
-        s.set_launch_plan(ends, blocks)
+        s.set_launch_plan(plan_ends, blocks)
         s.step(1)                                   # graphs and caches of this plan
         s.set_timing(True)
         s.step(steps)
@@ -130,10 +134,8 @@ def tune_buckets(prob, precision="fp32", candidates=(32, 64, 128, 256), steps=10
         s.set_timing(False)
         return t["step"][0] / steps
 
-    default = [0] * len(ends)
     default_block = 128 if len(prob.props) > 1 else 32
     pick = [default_block] * len(ends)
-    base = timed(pick)
     trials = {}
     for _ in range(rounds):
         for r in range(len(ends)):
@@ -141,16 +143,26 @@ def tune_buckets(prob, precision="fp32", candidates=(32, 64, 128, 256), steps=10
             for b in candidates:
                 trial = list(pick)
                 trial[r] = b
-                ms = timed(trial)
+                ms = timed(ends, trial)
                 trials[f"{buckets[r][0]}:{b}"] = ms
                 if verbose:
                     print(f"bucket {buckets[r][0]} block {b}: {ms:.4f} ms/step")
                 if best_t is None or ms < best_t:
                     best_b, best_t = b, ms
             pick[r] = best_b
-    final = timed(pick)
+    # merge adjacent buckets with the same block: one launch per range
+    plan = []
+    for r in range(len(ends)):
+        if plan and plan[-1][2] == pick[r]:
+            plan[-1] = (plan[-1][0], ends[r], pick[r])
+        else:
+            plan.append((buckets[r][0], ends[r], pick[r]))
+    p_ends, p_blocks = [e for _, e, _ in plan], [b for _, _, b in plan]
+    final = min(timed(p_ends, p_blocks) for _ in range(3))
+    base = min(timed([], []) for _ in range(3))
     s.set_launch_plan([], [])
     s.close()
-    del default
-    return {"plan": [(buckets[r][0], ends[r], pick[r]) for r in range(len(ends))], "step_ms": final,
-            "default_step_ms": base, "default_block": default_block, "trials": trials}
+    if len(plan) == 1 and plan[0][2] == default_block or not final < base:
+        plan, final = [], base
+    return {"plan": plan, "step_ms": final, "default_step_ms": base, "default_block": default_block,
+            "trials": trials}

@@ -828,6 +828,9 @@ def main():
                            "autotuned": bool(tuned), "dtime": prob.dtime,
                            "launch_plan": ([{"bucket_elements": bk, "end": e, "block": blk} for bk, e, blk in plan]
                                            if plan else None),
+                           **({"autotune_step_ms": {"plan": round(tuned["step_ms"], 4),
+                                                    "single_default_launch": round(tuned["default_step_ms"], 4)}}
+                              if tuned and "default_step_ms" in tuned else {}),
                            "prestrain": args.prestrain,
                            "l2": "working set > L2 (state, nodal arrays and connectivity "
                                  f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",

@@ -156,8 +156,10 @@ def test_launch_plan_by_size_bucket(oracle):
     """An ensemble concatenated by specimen size has one element range per
     size bucket; a launch plan gives each range its own block (here a
     different one per bucket) and the run equals the single launch's and
-    the oracle's.  The bucket autotuner times each bucket's candidates and
-    returns a plan no slower than the default block."""
+    the oracle's.  The bucket autotuner times each bucket's candidates,
+    merges adjacent buckets with the same pick into one range, and returns
+    a plan only if it beats the single default launch (else none): never
+    slower than the default."""
     p = P.ensemble(nspec=12, nsteps=400, emin=100, emax=3000, by_size=True)
     buckets = P.size_buckets(p)
     assert len(buckets) >= 3 and buckets[-1][1] == p.nelem
@@ -179,5 +181,8 @@ def test_launch_plan_by_size_bucket(oracle):
     assert np.abs(out["plan"][0] - out["one"][0]).max() <= 1e-10 * scale
     assert np.abs(out["plan"][1] - h_ref).max() <= 1e-6 * np.abs(h_ref).max()
     t = tune.tune_buckets(p, precision="fp32", steps=5, warmup=2)
-    assert [e for _, e, _ in t["plan"]] == ends
-    assert t["step_ms"] <= 1.10 * t["default_step_ms"], t
+    if t["plan"]:
+        pe, pb = [e for _, e, _ in t["plan"]], [b for _, _, b in t["plan"]]
+        assert pe[-1] == p.nelem and set(pe) <= set(ends) and pe == sorted(pe), t["plan"]
+        assert all(pb[r] != pb[r + 1] for r in range(len(pb) - 1)), t["plan"]
+    assert t["step_ms"] <= t["default_step_ms"], t
