@@ -382,6 +382,15 @@ class ExplicitSolid:
     def kernel_launches(self):
         return int(lib().sma_kernel_launches(self._ctx))
 
+    def launch_info(self):
+        """The element kernel's launch shape this context chose
+        (sma_launch_info): threads per block, variant, compact records."""
+        b, v, k = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().sma_launch_info(self._ctx, C.byref(b), C.byref(v), C.byref(k)))
+        names = {val: name for name, val in VARIANT.items()}
+        return {"block": int(b.value), "variant": names.get(int(v.value), int(v.value)),
+                "compact_records": bool(k.value)}
+
 
 def host_register(arr):
     """Page-lock a C-contiguous numpy array in place (sma_host_register), so

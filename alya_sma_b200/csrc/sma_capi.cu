@@ -1835,6 +1835,15 @@ void* sma_stream(sma_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int64_t sma_kernel_launches(sma_ctx* c) { return c ? c->launches : 0; }
 
+// the element kernel's launch shape this context chose
+int32_t sma_launch_info(sma_ctx* c, int32_t* block, int32_t* variant, int32_t* compact) {
+  if (!c || !block || !variant || !compact) return fail(SMA_ERR_ARG, "NULL argument");
+  *block = c->block;
+  *variant = c->variant;
+  *compact = c->compact ? 1 : 0;
+  return SMA_OK;
+}
+
 int32_t sma_eval_law160(int64_t n, const double* props, double e_mart, const double* d_F,
                         const double* d_tmp, const double* d_sdv_old, double* d_sdv_new,
                         double* d_pk2, int32_t* d_nr_flag, int32_t precision, void* stream) {

@@ -51,13 +51,39 @@ WORKLOADS = {"cantilever": "cantilever_400x40x40_hex08",
              "ensemble": "ensemble_256_specimens_hex08"}
 
 
-def default_block(prob, variant):
-    """The element block the library picks when none is given (its context
-    set-up rule): 256 pipelined, else 128 with per-element materials, 32
-    with one."""
-    if variant == "pipe":
-        return 256
-    return 128 if len(prob.props) > 1 else 32
+L2_BYTES = 126e6          # B200 L2
+
+
+def arm_config(args, world, nelem, npoin, gauss_points, wset_mesh):
+    """The workload the line is quoted on -- the same dict in the reference
+    arm's line as in this arm's: the mesh (nelem, npoin of the job's unique
+    mesh or meshes), its Gauss points over the whole job, the form, the
+    prestrain, the working set per GPU against L2 and how the job uses the
+    GPUs.  How this arm launches it (threads per block, scatter, tuning) is
+    in the line's `launch`."""
+    sharded = args.workload == "ensemble" and world > 1
+    split = bool(args.partition) and not sharded
+    per_gpu = wset_mesh / world if (sharded or split) else wset_mesh
+    if sharded:
+        par = f"specimens sharded over {world} GPUs (no exchange)"
+    elif split:
+        par = (f"one mesh in {world} element slabs, the shared nodes' residual rows exchanged with the "
+               "neighbouring slabs every step, overlapped with the interior elements")
+    else:
+        par = f"replicas x{world}" if world > 1 else "single GPU"
+    return {"workload": workload_name(args.workload, args.div), "nelem": int(nelem), "npoin": int(npoin),
+            "gauss_points": int(gauss_points), "precision": args.precision, "prestrain": args.prestrain,
+            "l2": (("working set > L2 (state, nodal arrays and connectivity "
+                    f"~{per_gpu / 1e6:.0f} MB per step per GPU vs 126 MB L2)") if per_gpu > L2_BYTES else
+                   (f"working set ~{per_gpu / 1e6:.0f} MB per GPU fits the 126 MB L2 (a test-sized mesh: "
+                    "its arrays stay cached between steps)")),
+            "parallelism": par}
+
+
+def working_set(prob, precision):
+    """Bytes one step streams: the element kernel's algorithmic bytes and the
+    nodal update's six FP64 nodal arrays read and written."""
+    return algorithmic_bytes(prob, precision) + 6 * 24 * prob.npoin
 
 
 def workload_name(workload, div):
@@ -71,7 +97,7 @@ def workload_name(workload, div):
     return f"{WORKLOADS[workload]}_coarsened_{div}x"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=400)
@@ -106,7 +132,7 @@ def parse():
                          "shared nodes' residual exchanged with the neighbouring slabs while the interior "
                          "elements compute): strong scaling.  Default: on for the cylinder and the "
                          "cantilever under --gpus N > 1, off at N = 1; the ensemble shards its specimens")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
@@ -470,7 +496,11 @@ def run_reference(args):
     if world > 1 and rank != 0:
         return 0
     from alya_sma_b200 import problem as P
+    if args.partition is None:
+        args.partition = world > 1 and args.workload != "ensemble"
     prob = build_problem(args.workload, args.div, layers=args.layers)
+    sharded = args.workload == "ensemble" and world > 1
+    gp_all = prob.nelem * 8 * (1 if (sharded or args.partition) else world)
     u0 = P.prestrain(prob, args.prestrain)
     base = cpu_baseline(prob, u0, budget_s=15.0, max_steps=max(2, args.steps))
     line = {"impl": "reference", "metric": "Gauss-point updates/s (explicit SMA step)",
@@ -479,9 +509,9 @@ def run_reference(args):
             "ms_per_step": prob.nelem * 8 / base["value"] * 1e3, "higher_is_better": True,
             "scaling": "strong" if (args.workload == "ensemble" and world > 1) else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(args.workload, args.div), "nelem": prob.nelem, "npoin": prob.npoin,
-                       "gauss_points": prob.nelem * 8, "precision": "fp64 (reference CPU path)",
-                       "prestrain": args.prestrain},
+            "config": arm_config(args, world, prob.nelem, prob.npoin, gp_all, working_set(prob, args.precision)),
+            "reference_path": "the oracle's FP64 restatement of the reference CPU step (the Fortran reference "
+                              "does not build here), OpenMP colour-parallel on the host cores",
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "GP-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -592,12 +622,9 @@ def run_partitioned(args, rank, world, local):
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32" else "f64",
                 "data": "synthetic",
-                "config": {"workload": workload_name(args.workload, args.div), "nelem": prob.nelem,
-                           "npoin": prob.npoin, "gauss_points": ngp, "precision": args.precision,
-                           "scatter": args.scatter, "prestrain": args.prestrain,
-                           "parallelism": f"one mesh in {world} element slabs, {ps.nshared} shared nodes "
-                                          "exchanged with the neighbouring slabs every step, overlapped with the "
-                                          "interior elements"},
+                "config": arm_config(args, world, prob.nelem, prob.npoin, ngp, working_set(prob, args.precision)),
+                "launch": {"scatter": args.scatter, **part.launch_info(), "dtime": prob.dtime,
+                           "shared_nodes": ps.nshared},
                 "roofline": roofline, "gpu_launches": launches, "clocks": ck, "e2e": e2e}
         print(json.dumps(line))
     ps.close()
@@ -662,6 +689,7 @@ def main():
                               device=local, variant=variant)
     if plan:
         solid.set_launch_plan([e for _, e, _ in plan], [blk for _, _, blk in plan])
+    launch_info = solid.launch_info()
     solid.set("displ", u0)
     stream = torch.cuda.ExternalStream(solid.stream)
     solid.step(max(3, args.warmup))
@@ -705,11 +733,15 @@ def main():
         physics["surrogate_network_refusal_fraction"] = cnt["sur_ood"] * SUR_PERIOD / (ngp * args.steps)
         physics["surrogate_training"] = sur_info
     ngp_all = world * ngp                                      # replicas: the same mesh per rank
+    nelem_all, npoin_all, wset_all = nelem, prob.npoin, working_set(prob, args.precision)
     from alya_sma_b200 import dist as D                       # (identity on one rank)
     if world > 1:
         ms = D.max_over_ranks(ms, "cuda")                      # the slowest rank sets the time
         if sharded:
             ngp_all = int(D.sum_over_ranks(ngp, "cuda"))       # each specimen counted once
+            nelem_all = int(D.sum_over_ranks(nelem, "cuda"))
+            npoin_all = int(D.sum_over_ranks(prob.npoin, "cuda"))
+            wset_all = float(D.sum_over_ranks(wset_all, "cuda"))
     value = ngp_all * args.steps / (ms / 1e3)
 
     # ---- per-kernel device times (roofline of the element kernel): the same
@@ -822,20 +854,13 @@ def main():
                 "scaling": "strong" if sharded else "weak", "vs_baseline": None,
                 "dtype": {"fp32": "f32+f64", "fp64": "f64", "surrogate": "bf16+f32+f64"}[args.precision],
                 "data": "synthetic",
-                "config": {"workload": workload_name(args.workload, args.div), "nelem": nelem, "npoin": prob.npoin,
-                           "gauss_points": ngp_all, "precision": args.precision,
-                           "scatter": args.scatter, "block": block or default_block(prob, variant), "variant": variant,
-                           "autotuned": bool(tuned), "dtime": prob.dtime,
+                "config": arm_config(args, world, nelem_all, npoin_all, ngp_all, wset_all),
+                "launch": {"scatter": args.scatter, **launch_info, "autotuned": bool(tuned), "dtime": prob.dtime,
                            "launch_plan": ([{"bucket_elements": bk, "end": e, "block": blk} for bk, e, blk in plan]
                                            if plan else None),
                            **({"autotune_step_ms": {"plan": round(tuned["step_ms"], 4),
                                                     "single_default_launch": round(tuned["default_step_ms"], 4)}}
-                              if tuned and "default_step_ms" in tuned else {}),
-                           "prestrain": args.prestrain,
-                           "l2": "working set > L2 (state, nodal arrays and connectivity "
-                                 f"~{(alg + 6 * 24 * prob.npoin) / 1e6:.0f} MB per step vs 126 MB L2)",
-                           "parallelism": (f"specimens sharded over {world} GPUs (no exchange)" if sharded
-                                           else f"replicas x{world}" if world > 1 else "single GPU")},
+                              if tuned and "default_step_ms" in tuned else {})},
                 "roofline": roofline, "gpu_launches": launches, "clocks": ck, "physics": physics}
         line.update(extras)
         print(json.dumps(line))

@@ -425,6 +425,12 @@ int32_t sma_set_launch_plan(sma_ctx* ctx, int32_t nrange, const int32_t* end, co
 /* kernel launches issued by this context since creation (all kernels) */
 int64_t sma_kernel_launches(sma_ctx* ctx);
 
+/* The element kernel's launch shape the context chose (no counterpart in the
+ * reference, whose element loop has no launch): threads per block, the
+ * SMA_VARIANT_* it runs, and 1 in *compact if per-element materials are read
+ * as compact records. */
+int32_t sma_launch_info(sma_ctx* ctx, int32_t* block, int32_t* variant, int32_t* compact);
+
 const char* sma_last_error(void);
 const char* sma_version(void);
 
