@@ -839,9 +839,34 @@ def main():
             sma._check(L.sma_assemble(ctx, dnp.ctypes.data, 0.0, rnp.ctypes.data, None, None, None, None))
             solid.end_step()
         te = D.max_over_ranks(time.perf_counter() - t0, "cuda")
+        # the host link alone: the same bytes copied from and to the same
+        # pinned buffers, both directions at once on two streams, the same
+        # number of times -- the floor the call's copies set
+        dd = torch.empty((npoin, 3), dtype=torch.float64, device=local)
+        dr = torch.empty((npoin, 3), dtype=torch.float64, device=local)
+        s_in, s_out = torch.cuda.Stream(local), torch.cuda.Stream(local)
+        for rep in range(2):                                  # one untimed round, one timed
+            barrier()
+            t1 = time.perf_counter()
+            for _ in range(ke):
+                with torch.cuda.stream(s_in):
+                    dd.copy_(hd, non_blocking=True)
+                with torch.cuda.stream(s_out):
+                    hr.copy_(dr, non_blocking=True)
+                s_in.synchronize()
+                s_out.synchronize()
+            tl = time.perf_counter() - t1
+        tl = D.max_over_ranks(tl, "cuda")
+        del dd, dr
         extras["e2e"] = {"value": ngp_all * ke / te, "unit": "GP-updates/s",
                          "h2d_bytes_per_step": 3 * npoin * 8, "d2h_bytes_per_step": 3 * npoin * 8,
-                         "boundary": "sma_assemble (element loop, host displ in, host rhsid out)"}
+                         "boundary": "sma_assemble (element loop, host displ in, host rhsid out)",
+                         "ms_per_step": round(te / ke * 1e3, 4),
+                         "host_link": {"copies_ms_per_step": round(tl / ke * 1e3, 4),
+                                       "gb_s_each_way": round(3 * npoin * 8 / (tl / ke) / 1e9, 1),
+                                       "frac": round(tl / te, 3),
+                                       "what": "pinned copies of the same bytes, both directions at once, "
+                                               "no kernels: the floor of the call's time"}}
         if world == 1:
             extras["cpu_baseline"] = cpu_baseline(prob, u0)
     if world > 1:
