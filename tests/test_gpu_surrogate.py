@@ -284,3 +284,33 @@ def test_network_gain_over_the_analytic_part_alone(oracle):
     g64.close()
     assert err["network"][0] < 1e-3, err
     assert err["network"][0] < 0.5 * err["zero"][0] and err["network"][1] < err["zero"][1], err
+
+
+def test_surrogate_switch_rejects_and_restores(oracle):
+    """sma_set_surrogate's contract: the FP64 form, the coloured scatter and
+    out-of-range gates are rejected before any device work; switched off
+    (enable = 0) the context's element loop is the plain FP32 law again, bit
+    for bit."""
+    import alya_sma_b200 as sma
+    net, _ = _trained(npath=512, epochs=1)
+    p = P.bar_40x4x4(nsteps=100)
+    u = np.zeros_like(p.coord)
+    u[:, 0] = 0.02 * p.coord[:, 0]
+    for kw in ({"precision": "fp64"}, {"precision": "fp32", "scatter": "color"}):
+        g = sma.ExplicitSolid(p, **kw)
+        with pytest.raises(sma.SmaError):
+            g.set_surrogate(net)
+        g.close()
+    g = sma.ExplicitSolid(p, precision="fp32")
+    for bad in ({"gate": 0.0}, {"xs_tol": -1.0}, {"f_margin": -1.0}, {"period": 0}):
+        with pytest.raises(sma.SmaError):
+            g.set_surrogate(net, **bad)
+    plain = g.assemble(u)["finte"]
+    g.set_surrogate(net)
+    with_sur = g.assemble(u)["finte"]
+    g.set_surrogate(net, enable=False)
+    again = g.assemble(u)["finte"]
+    g.close()
+    assert np.array_equal(again, plain)
+    assert not np.array_equal(with_sur, plain)
+    assert np.abs(with_sur - plain).max() <= 1e-3 * np.abs(plain).max()
