@@ -867,6 +867,26 @@ def main():
                                        "frac": round(tl / te, 3),
                                        "what": "pinned copies of the same bytes, both directions at once, "
                                                "no kernels: the floor of the call's time"}}
+        # the step boundary (sma_explicit_step): the state stays on the
+        # device; the host asks for K steps and reads back, as the step's
+        # result, the axial displacement history of the far face's first node
+        # (the witness rows, one per step); wall time around the calls
+        far = int(np.flatnonzero(np.isclose(prob.coord[:, 0], prob.coord[:, 0].max()))[0])
+        solid.set_witness([3 * far], args.steps)
+        solid.step(2)
+        solid.witness()
+        solid.set_witness([3 * far], args.steps)
+        barrier()
+        t0 = time.perf_counter()
+        solid.step(args.steps)
+        hist = solid.witness()
+        ts = D.max_over_ranks(time.perf_counter() - t0, "cuda")
+        assert hist.shape[0] == args.steps and np.isfinite(hist).all()
+        extras["e2e_step_boundary"] = {"value": ngp_all * args.steps / ts, "unit": "GP-updates/s",
+                                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
+                                       "ms_per_step": round(ts / args.steps * 1e3, 4),
+                                       "boundary": "sma_explicit_step over the K steps (state resident), the "
+                                                   "far-face displacement history read back"}
         if world == 1:
             extras["cpu_baseline"] = cpu_baseline(prob, u0)
     if world > 1:
