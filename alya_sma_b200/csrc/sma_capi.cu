@@ -499,6 +499,26 @@ int32_t launch_sur_refresh(sma_ctx* c, int cls) {
   return SMA_OK;
 }
 
+// the held residual of every point from the network at the TIME_N state and
+// the current displacement, one residue class of tiles at a time: at
+// switch-on, and when the caller replaces the state or the displacement
+int32_t sur_init_residuals(sma_ctx* c) {
+  CU(cudaMemsetAsync(c->d_rcache, 0xff, 6 * (size_t)c->sst * sizeof(__half), c->stream));   // NaN: none held
+  ElemArgs<float> a = elem_args<float>(c, 0, c->nelem, false, false);
+  const sur::SurElemArgs sa = sur_args(c);
+  const int64_t ntiles = ceil_div(c->nelem, sur::SUR_EPB);
+  for (int cls = 0; cls < c->sur_period && cls < ntiles; ++cls) {
+    const unsigned grid = (unsigned)ceil_div(ntiles - cls, c->sur_period);
+    if (c->compact) sur::k_sur_stage<true><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
+    else sur::k_sur_stage<false><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
+    c->launches++;
+    CU(cudaGetLastError());
+    int32_t rc = launch_sur_refresh(c, cls);
+    if (rc) return rc;
+  }
+  return SMA_OK;
+}
+
 // the element loop by the launch plan: range r with its own block size (the
 // one-tile kernel, narrow or wide instance by block)
 template <typename T>
@@ -1508,6 +1528,9 @@ int32_t sma_set_nodal(sma_ctx* c, int32_t field, const double* host) {
   k_aos_to_soa<<<(unsigned)ceil_div(c->npoin, 256), 256, 0, c->stream>>>(c->d_stage, dst, c->npoin, c->npad);
   c->launches++;
   CU(cudaGetLastError());
+  // the surrogate's held residuals belong to the displacement they were taken at
+  int32_t rc;
+  if (field == SMA_FIELD_DISPL && c->sur && (rc = sur_init_residuals(c))) return rc;
   CU(cudaStreamSynchronize(c->stream));
   return SMA_OK;
 }
@@ -1573,7 +1596,15 @@ static int32_t state_io(sma_ctx* c, double* host, bool in) {
   return SMA_OK;
 }
 
-int32_t sma_set_state(sma_ctx* c, const double* host) { return state_io(c, const_cast<double*>(host), true); }
+int32_t sma_set_state(sma_ctx* c, const double* host) {
+  int32_t rc = state_io(c, const_cast<double*>(host), true);
+  // the surrogate's held residuals belong to the state they were taken at
+  if (!rc && c->sur) {
+    if ((rc = sur_init_residuals(c))) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+  }
+  return rc;
+}
 int32_t sma_get_state(sma_ctx* c, double* host) { return state_io(c, host, false); }
 
 int32_t sma_get_time(sma_ctx* c, double* cutim) {
@@ -2139,21 +2170,7 @@ extern "C" int32_t sma_set_surrogate(sma_ctx* c, const float* params, const sma_
   sur::k_sur_pack_image<<<(sur::HID * sur::HID + 255) / 256, 256, 0, c->stream>>>(d_w, c->d_sur_img);
   CU(cudaMemcpyAsync(c->d_sur_stats, stats, sizeof(sur::SurStats), cudaMemcpyHostToDevice, c->stream));
   CU(cudaMemsetAsync(c->d_sur_ctr, 0, 2 * sizeof(int), c->stream));
-  CU(cudaMemsetAsync(c->d_rcache, 0xff, 6 * (size_t)c->sst * sizeof(__half), c->stream));   // NaN: none held
-  // the first residual of every point: the network on the TIME_N state at
-  // the current displacement, one residue class of tiles at a time
-  {
-    ElemArgs<float> a = elem_args<float>(c, 0, c->nelem, false, false);
-    const sur::SurElemArgs sa = sur_args(c);
-    for (int cls = 0; cls < period && cls < ntiles; ++cls) {
-      const unsigned grid = (unsigned)ceil_div(ntiles - cls, period);
-      if (c->compact) sur::k_sur_stage<true><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
-      else sur::k_sur_stage<false><<<grid, sur::SUR_BLOCK, 0, c->stream>>>(a, sa, cls);
-      CU(cudaGetLastError());
-      if ((rc = launch_sur_refresh(c, cls))) return rc;
-    }
-  }
-  CU(cudaGetLastError());
+  if ((rc = sur_init_residuals(c))) return rc;
   CU(cudaStreamSynchronize(c->stream));
   if (!stage) cudaFree(d_w);
   destroy_graphs(c);

@@ -324,8 +324,9 @@ int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats
  * keep xS; the transformation strain is eL xS on the current strain
  * direction, as the law keeps it.  params: SMA_SUR_NPARAM host FP32
  * values, stats: host.  Switching on evaluates the network once on every
- * point at the TIME_N state and the current displacement; enable = 0
- * returns to the plain law.  A step with the surrogate launches the element
+ * point at the TIME_N state and the current displacement, and so does
+ * replacing either while it is on (sma_set_state, sma_checkpoint_load,
+ * sma_set_nodal of the displacement); enable = 0 returns to the plain law.  A step with the surrogate launches the element
  * kernel and the network kernel.  Counters: slot 5 (SMA_CNT_SUR_FALLBACK)
  * Gauss points the plain law handled, slot 7 (SMA_CNT_SUR_OOD) network
  * evaluations its gates refused. */

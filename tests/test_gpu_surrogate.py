@@ -314,3 +314,30 @@ def test_surrogate_switch_rejects_and_restores(oracle):
     assert np.array_equal(again, plain)
     assert not np.array_equal(with_sur, plain)
     assert np.abs(with_sur - plain).max() <= 1e-3 * np.abs(plain).max()
+
+
+def test_surrogate_follows_a_replaced_state(oracle):
+    """The held residuals belong to the state and displacement they were
+    taken at: switching the surrogate on and then replacing both gives the
+    element forces of switching it on after them (to the atomic scatter's
+    summation order)."""
+    import alya_sma_b200 as sma
+    net, _ = _trained(npath=512, epochs=1)
+    p = P.cylinder_2m(nsteps=600, div=8)
+    g64 = sma.ExplicitSolid(p, precision="fp64")
+    g64.set("displ", P.prestrain(p, 0.01))
+    g64.step(30)
+    u, state = g64.get("displ"), g64.state
+    g64.close()
+    out = []
+    for first in (True, False):
+        g = sma.ExplicitSolid(p, precision="fp32")
+        if first:
+            g.set_surrogate(net)
+        g.state = state
+        g.set("displ", u)
+        if not first:
+            g.set_surrogate(net)
+        out.append(g.assemble(u)["finte"])
+        g.close()
+    assert np.abs(out[0] - out[1]).max() <= 1e-12 * np.abs(out[1]).max()
