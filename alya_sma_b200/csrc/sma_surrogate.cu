@@ -177,4 +177,18 @@ int32_t sma_sur_forward(const unsigned char* d_img, const sma_sur_stats* d_stats
   return SMA_OK;
 }
 
+int32_t sma_sur_wait_check(int32_t tries, int32_t* status) {
+  if (!status) return sfail(SMA_ERR_ARG, "NULL argument");
+  if (tries < 1 || tries > (1 << 20)) return sfail(SMA_ERR_ARG, "tries in [1, 2^20]");
+  int* d = nullptr;
+  SCU(cudaMalloc(&d, sizeof(int)));
+  SCU(cudaMemset(d, 0xff, sizeof(int)));
+  sur::k_sur_wait_check<<<1, 32>>>(tries, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return sfail(SMA_ERR_CUDA, cudaGetErrorString(e));
+  return SMA_OK;
+}
+
 }  // extern "C"

@@ -789,6 +789,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int l
   }
   return false;
 }
+// The bounded wait on its own: thread 0 initialises an mbarrier that
+// nothing arrives at and waits for its first phase, `tries` tries -- the path
+// a network kernel takes if its tensor-core work never completes.
+// status = 1 if the wait gave up (the expected answer), 0 if it saw the phase
+// complete.
+static __global__ void k_sur_wait_check(int tries, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *status = mbar_wait(&bar, 0u, tries) ? 0 : 1;
+  }
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

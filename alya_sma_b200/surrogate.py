@@ -41,8 +41,17 @@ def _bind():
     L.sma_sur_adam.argtypes = [vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp]
     L.sma_sur_pack.argtypes = [vp, vp, vp, vp]
     L.sma_sur_forward.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp]
+    L.sma_sur_wait_check.argtypes = [i32, C.POINTER(C.c_int32)]
     L._sur_bound = True
     return L
+
+
+def wait_check(tries=1000):
+    """sma_sur_wait_check: 1 if the network kernels' bounded mbarrier wait
+    gives up on a phase that never completes (as it must), 0 otherwise."""
+    st = C.c_int32(-1)
+    _check(_bind().sma_sur_wait_check(int(tries), C.byref(st)))
+    return int(st.value)
 
 
 def generate(props, e_mart, npath, nstep=512, seed=0, spread=0.10, t_range=(300.0, 320.0),

@@ -337,6 +337,12 @@ int32_t sma_set_surrogate(sma_ctx* ctx, const float* params, const sma_sur_stats
 /* 1 in *status if a wait of the surrogate's network kernel for the tensor
  * cores ran out since it was switched on (never expected), else 0. */
 int32_t sma_surrogate_status(sma_ctx* ctx, int32_t* status);
+/* Check of the bounded wait the network kernels use for their tensor-core
+ * work (no counterpart in the reference): one kernel waits, `tries` tries
+ * (1..2^20), for an mbarrier phase that nothing completes.  *status = 1
+ * when the wait gave up, as it must; 0 would mean it saw a phase complete.
+ * Synchronises the device. */
+int32_t sma_sur_wait_check(int32_t tries, int32_t* status);
 
 /* host <-> context data */
 int32_t sma_set_nodal(sma_ctx* ctx, int32_t field, const double* host);
