@@ -82,20 +82,6 @@ __device__ __forceinline__ float2 unpack_bf16(uint32_t u) {
   return __bfloat1622float2(v);
 }
 
-// linear-elastic stress over E of the strain e (nu through kK = 1/(3-6nu),
-// kG = 1/(2+2nu): lambda/E = kK - 2 kG / 3, 2 mu/E = 2 kG)
-template <typename T>
-__device__ __forceinline__ void lin_elastic(double kK, double kG, const T* e, T* s) {
-  const T lam = (T)(kK - 2.0 * kG / 3.0), mu2 = (T)(2.0 * kG);
-  const T tr = lam * (e[0] + e[1] + e[2]);
-  s[0] = tr + mu2 * e[0];
-  s[1] = tr + mu2 * e[1];
-  s[2] = tr + mu2 * e[2];
-  s[3] = mu2 * e[3];
-  s[4] = mu2 * e[4];
-  s[5] = mu2 * e[5];
-}
-
 // The analytic part of the response.  h = E - E^2 + 4/3 E^3 is ln U to
 // O(E^4) (E the Green-Lagrange strain, C = I + 2E).  The law's transformation
 // strain always lies along the current deviatoric direction with length
