@@ -413,24 +413,35 @@ def surrogate_leg(args, prob, u0, s64, v64, v32, wsteps, device, spread=None):
     g = sma.ExplicitSolid(prob, precision="fp32", scatter=args.scatter, device=device)
     g.set("displ", u0)
     g.step(wsteps)
-    # one element loop at the switch-on state judged by the plain FP64 law,
-    # with the network and with its output held at zero (the method without
-    # the learned part)
+    # one element loop judged by the plain FP64 law at the same state and
+    # displacement (the FP64 run's after the warm-up steps, loaded into an
+    # FP32 context), with the network and with its output held at zero (the
+    # method without the learned part)
     j64 = sma.ExplicitSolid(prob, precision="fp64", scatter=args.scatter, device=device)
     j64.set("displ", u0)
     j64.step(wsteps)
-    f64 = j64.assemble(j64.get("displ"))["finte"]
+    uj, sj = j64.get("displ"), j64.state
+    f64 = j64.assemble(uj)["finte"]
     j64.close()
     fscale = float(np.abs(f64).max())
-    judged = {"what": "nodal internal forces of one surrogate element loop at the switch-on state vs the plain "
-                      "FP64 law's, relative to the largest; zero_residual: the same loop with the network's "
-                      "output held at zero (the analytic part alone)"}
+    judged = {"what": "nodal internal forces of one surrogate element loop vs the plain FP64 law's at the same "
+                      "state and displacement (the FP64 run's after the warm-up steps), relative to the largest; "
+                      "zero_residual: the same loop with the network's output held at zero (the analytic part "
+                      "alone)"}
+    gj = sma.ExplicitSolid(prob, precision="fp32", scatter=args.scatter, device=device)
+    gj.state = sj
+    gj.set("displ", uj)
     for name, n in (("zero_residual", S.ZeroResidual(net)), ("network", net)):
-        g.set_surrogate(n, gate=args.surrogate_gate, xs_tol=1e-3, period=SUR_PERIOD)
-        d = np.abs(g.assemble(g.get("displ"))["finte"] - f64).max(axis=1) / fscale
+        gj.set_surrogate(n, gate=args.surrogate_gate, xs_tol=1e-3, period=SUR_PERIOD)
+        d = np.abs(gj.assemble(uj)["finte"] - f64).max(axis=1) / fscale
         judged[name] = {"force_rel_max": float(d.max()), "force_rel_q9999": float(np.quantile(d, 0.9999)),
                         "force_rel_median": float(np.median(d))}
-    del f64
+    gj.set_surrogate(net, enable=False)
+    d = np.abs(gj.assemble(uj)["finte"] - f64).max(axis=1) / fscale
+    judged["fp32_plain_law"] = {"force_rel_max": float(d.max()), "force_rel_q9999": float(np.quantile(d, 0.9999)),
+                                "force_rel_median": float(np.median(d))}
+    gj.close()
+    del f64, sj
     g.set_surrogate(net, gate=args.surrogate_gate, xs_tol=1e-3, period=SUR_PERIOD)
     g.counters(reset=True)
     st = torch.cuda.ExternalStream(g.stream)
