@@ -89,3 +89,27 @@ def test_no_device_is_an_error_not_a_fallback():
         pytest.skip("a CUDA device is present")
     with pytest.raises(sma.SmaError, match="device"):
         sma.ExplicitSolid(_prob())
+
+
+def test_surrogate_entry_points_reject_bad_input_before_the_device():
+    """The surrogate's C-ABI calls check their arguments on the host first:
+    NULL pointers, empty batches, an unaligned weight image, an out-of-range
+    wait limit and a NULL context come back as SMA_ERR_ARG with no device
+    call."""
+    from alya_sma_b200 import surrogate as S
+    ERR_ARG = -1                                   # SMA_ERR_ARG, include/alya_sma.h
+    L = S._bind()
+    st = C.c_int32(-1)
+    assert L.sma_sur_wait_check(0, C.byref(st)) == ERR_ARG
+    assert L.sma_sur_wait_check(1 << 21, C.byref(st)) == ERR_ARG
+    assert L.sma_sur_wait_check(10, None) == ERR_ARG
+    assert L.sma_sur_forward(None, None, 0, None, None, None, None, None) == ERR_ARG
+    assert L.sma_sur_forward(C.c_void_p(16), C.c_void_p(16), 8, None, None, None, None, None) == ERR_ARG
+    assert L.sma_sur_forward(C.c_void_p(17), C.c_void_p(16), 8, C.c_void_p(16), C.c_void_p(16), None,
+                             C.c_void_p(16), None) == ERR_ARG
+    assert b"aligned" in L.sma_last_error()
+    L.sma_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                    C.c_int32, C.c_int32]
+    assert L.sma_set_surrogate(None, None, None, 3.0, 1e-3, 10.0, 64, 1) == ERR_ARG
+    L.sma_launch_info.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    assert L.sma_launch_info(None, None, None, None) == ERR_ARG
